@@ -1,0 +1,372 @@
+"""Benchmark of the M^+M CG hot path on B200 (one JSON line on rank 0).
+
+Workload (the 32^3 x 64 configuration): clover-Wilson, c_sw = 1.9192,
+kappa = 0.13, antiperiodic in t; links = seeded hot start (BQCD's ranf, default
+seed) + 10 sweeps of conf_relax cooling, all generated on the device; b =
+ran_gauss_volh(12, b, 1/2, EVEN) (unit-variance complex).  A step is one solve
+of M~^+M~ x = b from x = 0 to a true FP64 |r|/|b| < 1e-10:
+  value   mixed-precision CG (int16 sloppy fields, FP64 reliable updates), s
+  fp64    the all-FP64 CG on the same system (same kernels, FP64 storage)
+  e2e     the reference-facing C-ABI call with host arrays: links (flipped, as
+          at BQCD's call sites), clover A and A^-1, b and x uploaded and x
+          downloaded inside the timed region
+Every field is larger than the 126 MB L2 (spinor 201 MB FP64, links 1.2 GB),
+so no L2 flush is needed between steps.
+
+--impl reference times the CPU restatement of the reference's CG (OpenMP, all
+host threads) on a bounded sample of iterations of the same system.
+Multi-GPU (torchrun): independent replicas, one solve per GPU, no collective in
+the data path; the step time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "bqcd-r399-quda_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "M†M CG time-to-1e-10 at 32^3x64: mixed vs FP64 (1 B200); D-slash HBM GB/s"
+KAPPA, CSW, COOL = 0.13, 1.9192, 10
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.out:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if _has_cuda() else "gloo", timeout=datetime.timedelta(seconds=600),
+                                device_id=None)
+        pg = dist
+    return world, rank, local, pg
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        if _has_cuda():
+            torch.cuda.set_device(local)
+        pg.barrier()
+
+
+def allmax(pg, v, local):
+    if pg is None:
+        return v
+    import torch
+    dev = torch.device("cuda", local) if _has_cuda() else torch.device("cpu")
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_system(bq, L, device, seed_skip):
+    lat = bq.Lattice(L, (1, 1, 1, -1), device=device)
+    lat.ranset(0)
+    lat.conf_hot()
+    lat.conf_relax(COOL)
+    lat.clover_init(CSW * KAPPA)
+    lat.ranset(0, seed_skip)
+    hb = lat.field()
+    lat.field_gauss(hb, 0.5)
+    hx = lat.field()
+    return lat, hb, hx
+
+
+def stencil_bytes_per_site(prec):
+    """Algorithmic bytes of one mtil first-half pass (D_oe + Ainv_oo) per odd
+    output site: read the input spinor once, 8 links, one clover block, write
+    one spinor.  int16 fields carry one 4-byte norm per spinor/clover site."""
+    if prec == 0:
+        s, gl, c = 192, 144, 576          # FP64, 18-real links
+    elif prec == 1:
+        s, gl, c = 96, 48, 288            # FP32, 12-real links
+    else:
+        s, gl, c = 52, 24, 148            # int16 + norm, 12-real links
+    return 2 * s + 8 * gl + c
+
+
+def run_ours(args):
+    import numpy as np
+    import bqcdg as bq
+
+    world, rank, local, pg = dist_init()
+    L = tuple(int(x) for x in args.lattice.split(","))
+    peak, peak_kind = peaks()
+    lat, hb, hx = build_system(bq, L, local, 1000003 * rank)
+    para = bq.HmcPara(kappa=KAPPA, csw=CSW)
+    zero = np.zeros((lat.volh, 3, 4), np.complex128)
+    plaq = 1.0 - lat.plaq_energy()
+
+    def solve(prec, timek=False):
+        lat.field_set(hx, zero)
+        return lat.solve_dev(hx, hb, para, precision=prec, tol=args.tol, relative=True, time_kernels=timek)
+
+    # warm-up (untimed): both solvers, builds the sloppy copies
+    for _ in range(args.warmup):
+        solve(bq.PREC_HALF)
+    fp64_warm = solve(bq.PREC_DOUBLE)
+
+    # timed region: K mixed-precision solves
+    barrier(pg, local)
+    infos = []
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            infos.append(solve(bq.PREC_HALF, timek=True))
+        wall = time.perf_counter() - t0
+    dev_s = sum(i.seconds for i in infos)
+    step_s = allmax(pg, dev_s / args.steps, local)
+    ok = all(i.converged for i in infos)
+
+    # FP64 baseline solves (same system, same kernels in FP64)
+    fp64 = [solve(bq.PREC_DOUBLE, timek=True) for _ in range(max(1, args.fp64_steps))]
+    fp64_s = allmax(pg, sum(i.seconds for i in fp64) / len(fp64), local)
+
+    # roofline of the dominant stencil kernel, from the CUDA events of the timed solves
+    st_ms = sum(i.stencil_ms for i in infos) / max(1, sum(i.stencil_launches for i in infos))
+    st_bytes = stencil_bytes_per_site(2) * lat.volh
+    st_gbs = st_bytes / (st_ms * 1e-3) / 1e9
+    f64_ms = sum(i.stencil_ms for i in fp64) / max(1, sum(i.stencil_launches for i in fp64))
+    f64_gbs = stencil_bytes_per_site(0) * lat.volh / (f64_ms * 1e-3) / 1e9
+
+    # e2e through the reference-facing call (host arrays, transfers timed)
+    e2e = None
+    if not args.no_e2e:
+        u_host = lat.get_gauge(flipped=True)
+        a_host, i_host, _ = lat.get_clover()
+        b_host = lat.field_get(hb)
+        x_host = np.zeros_like(b_host)
+        lat2 = lat
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        lat2.load_gauge(u_host, flipped=True)
+        lat2.load_clover(a_host, i_host, None)
+        x, einfo = lat2.solve(x_host, b_host, para, precision=bq.PREC_HALF, tol=args.tol)
+        e2e_s = allmax(pg, time.perf_counter() - t0, local)
+        h2d = u_host.nbytes + a_host.nbytes + i_host.nbytes + b_host.nbytes + x_host.nbytes
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(x.nbytes),
+               "converged": bool(einfo.converged)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(lat, hb, L, fp64[0].niter, args.cpu_seconds)
+
+    if rank == 0:
+        it = infos[-1]
+        flops_site_iter = 4 * 1824          # 4 clover D-slash applications per M^+M (north_star convention)
+        gflops = flops_site_iter * lat.volh * it.niter / step_s / 1e9
+        out = {
+            "metric": METRIC,
+            "value": round(step_s, 6),
+            "unit": "s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(step_s * 1e3, 3),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64 (int16/f32 sloppy iterations)",
+            "data": "synthetic: device hot start (BQCD ranf, default seed) + %d cooling sweeps, Gaussian b" % COOL,
+            "config": {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
+                                   % ("x".join(map(str, L)), KAPPA, CSW),
+                       "lattice": list(L), "volh": lat.volh, "plaquette": round(plaq, 6),
+                       "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 (no flush)"},
+            "mixed": {"time_s": step_s, "iterations": it.niter, "reliable_updates": it.reliable_updates,
+                      "true_rel_residual": (it.true_rtr / it.b2) ** 0.5, "converged": ok,
+                      "gflops": round(gflops, 1), "wall_s_per_step": wall / args.steps},
+            "fp64": {"time_s": fp64_s, "iterations": fp64[0].niter,
+                     "true_rel_residual": (fp64[0].true_rtr / fp64[0].b2) ** 0.5,
+                     "dslash_gbs": round(f64_gbs, 1), "dslash_frac": round(f64_gbs / peak, 4)},
+            "speedup_mixed_vs_fp64": round(fp64_s / step_s, 3),
+            "roofline": {"bound": "hbm", "achieved": round(st_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(st_gbs / peak, 4), "traffic": None,
+                         "kernel": "k_pass1<F16> (D_oe + Ainv_oo, int16 fields)",
+                         "bytes_per_launch": st_bytes, "avg_launch_ms": round(st_ms, 5), "peak_kind": peak_kind},
+            "e2e": e2e,
+            "gpu_launches": int(sum(i.kernel_launches for i in infos)),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    lat.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def cpu_baseline(lat, hb, L, fp64_iters, seconds):
+    """The oracle's FP64 CG (restated cg.F90, OpenMP on all host threads) on a
+    bounded sample of iterations of the same system; time-to-solution scaled
+    by the FP64 iteration count of the same algorithm."""
+    import numpy as np
+    from oracle import oracle as O
+    g = O.Geom(L, (1, 1, 1, -1))
+    u = lat.get_gauge(flipped=True)
+    a, ai, b = lat.get_clover()
+    bvec = lat.field_get(hb)
+    x = np.zeros_like(bvec)
+    # one iteration to size the sample
+    t0 = time.perf_counter()
+    g.cg("mtdagmt", x, bvec, u, (a, ai, b), KAPPA, CSW * KAPPA, 0.0, 0.0, rest=0.0, maxiter=1, log=2)
+    t1 = time.perf_counter() - t0
+    n = max(2, min(200, int(seconds / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    g.cg("mtdagmt", x, bvec, u, (a, ai, b), KAPPA, CSW * KAPPA, 0.0, 0.0, rest=0.0, maxiter=n, log=2)
+    dt = time.perf_counter() - t0
+    per_iter = dt / n
+    return {"value": per_iter * fp64_iters, "unit": "s", "cores": O.threads(), "kind": "port",
+            "sample": "%d FP64 CG iterations (cg.F90 restated, M~^+M~ at %s) = %.2f s; %.4f s/iteration x %d "
+                      "iterations of the FP64 GPU CG" % (n, "x".join(map(str, L)), dt, per_iter, fp64_iters)}
+
+
+def run_reference(args):
+    """CPU restatement of the reference's CG path on the host cores."""
+    import numpy as np
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    L = tuple(int(x) for x in args.lattice.split(","))
+    g = O.Geom(L, (1, 1, 1, -1))
+    O.ranset(0)
+    u = g.hot()
+    g.relax(u, COOL)
+    clov = g.clover_init(u, CSW * KAPPA)
+    g.flip_bc(u)
+    O.ranset(0)
+    b = g.gauss_spinor(0, 0.5)
+    # iterations to 1e-10 of the same FP64 algorithm (one full CPU solve)
+    b2 = float(np.vdot(b, b).real)
+    rest = np.float32(1e-20 * b2)
+    t0 = time.perf_counter()
+    _, iters, rtr, _ = g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=rest,
+                            maxiter=args.ref_maxiter, log=2)
+    full = time.perf_counter() - t0
+    per_iter = full / max(1, iters)
+    steps = []
+    for k in range(args.warmup + args.steps):
+        n = max(2, min(iters, int(args.cpu_seconds / max(per_iter, 1e-9))))
+        t0 = time.perf_counter()
+        g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=0.0, maxiter=n, log=2)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            steps.append(dt / n * iters)
+    v = sum(steps) / len(steps)
+    out = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (same generators on the host)", "impl": "reference",
+           "config": {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
+                                  % ("x".join(map(str, L)), KAPPA, CSW), "lattice": list(L)},
+           "cpu_baseline": {"value": v, "unit": "s", "cores": O.threads(), "kind": "port",
+                            "sample": "full solve: %d iterations in %.1f s; each step times a bounded sample of "
+                                      "iterations and scales to %d" % (iters, full, iters)},
+           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-maxiter", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,387 @@
+"""Python host mirror of BQCD's fermion hot path on the B200 library.
+
+The routines keep the reference's names and argument meaning (d, d_dag,
+clover_mult_a/ao/b, mtil, mtil_dag, mtdagmt, w_mult, w_mult_dag, w_dagger_w,
+cg, quda_solver, dsf, clover_dsf, clover_dsd, clover_init, clover_action) and
+call the CUDA library lib/libbqcdg.so through its C ABI (include/bqcdg.h).
+There is no fallback: without the built library or a GPU every call raises.
+
+Array conventions (numpy, C order, the Fortran memory layouts of defs.h):
+  spinor  complex128 (volh, 3, 4)        SPINCOL_FIELD  [site][colour][spin]
+  gauge   complex128 (4, 2, volh, 3, 3)  GAUGE_FIELD    [mu][eo][site][col][row]
+  clover  complex128 (2, volh, 2, 18)    CLOVER_FIELD_A/B [eo][site][chi][slot]
+  p       float64    (4, 2, volh, 8)     GENERATOR_FIELD
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "..", "lib", "libbqcdg.so")
+
+OK, EINVAL, ECUDA, ENOCONV, ENAN, ENOGAUGE, ENOCLOVER, ENOMEM, EUNSUPPORTED, ENOTSU3, ENODEVICE = range(11)
+PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
+EVEN, ODD = 0, 1
+
+
+class BqcdgError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__("%s: %s (status %d)" % (what, _lib_handle().bqcdg_error_string(status).decode(), status))
+
+
+class Params(C.Structure):
+    """bqcdg_params: kappa, csw_kappa, h, rho (type(hmc_para) subset)."""
+    _fields_ = [("kappa", C.c_double), ("csw_kappa", C.c_double), ("h", C.c_double), ("rho", C.c_double)]
+
+
+class CgPara(C.Structure):
+    """bqcdg_cg_para = type(type_cg_para) (cg.F90:30-34)."""
+    _fields_ = [("rest", C.c_float), ("maxiter", C.c_int), ("log", C.c_int)]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("maxiter", C.c_int), ("relative", C.c_int), ("tol", C.c_double),
+                ("delta", C.c_double), ("check_true_residual", C.c_int), ("time_kernels", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("niter", C.c_int), ("reliable_updates", C.c_int), ("rtr", C.c_double), ("true_rtr", C.c_double),
+                ("b2", C.c_double), ("seconds", C.c_double), ("stencil_ms", C.c_double),
+                ("stencil_launches", C.c_int), ("converged", C.c_int), ("kernel_launches", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_LIB = None
+
+
+def _lib_handle():
+    global _LIB
+    if _LIB is None:
+        path = os.path.abspath(LIBPATH)
+        if not os.path.exists(path):
+            raise RuntimeError("libbqcdg.so is not built (%s); run bqcd-r399-quda_b200/build.py" % path)
+        L = C.CDLL(path)
+        vp, ip, dp, i = C.c_void_p, C.c_void_p, C.c_void_p, C.c_int
+        P = C.POINTER
+        L.bqcdg_error_string.restype = C.c_char_p
+        L.bqcdg_error_string.argtypes = [i]
+        L.bqcdg_create.argtypes = [P(vp), P(C.c_int), P(C.c_int), i]
+        L.bqcdg_destroy.argtypes = [vp]
+        L.bqcdg_volh.argtypes = [vp]
+        L.bqcdg_device_bytes.argtypes = [vp]
+        L.bqcdg_device_bytes.restype = C.c_longlong
+        L.bqcdg_load_gauge.argtypes = [vp, dp, i]
+        L.bqcdg_get_gauge.argtypes = [vp, dp, i]
+        L.bqcdg_load_clover.argtypes = [vp, dp, dp, dp]
+        L.bqcdg_get_clover.argtypes = [vp, dp, dp, dp]
+        L.bqcdg_clover_init.argtypes = [vp, C.c_double]
+        L.bqcdg_clover_action.argtypes = [vp, i, P(C.c_double)]
+        for n in ("bqcdg_d", "bqcdg_d_dag"):
+            getattr(L, n).argtypes = [vp, i, i, dp, dp]
+        L.bqcdg_clover_mult_a.argtypes = [vp, i, dp, dp]
+        L.bqcdg_clover_mult_ao.argtypes = [vp, i, dp]
+        L.bqcdg_clover_mult_b.argtypes = [vp, i, dp]
+        for n in ("bqcdg_mtil", "bqcdg_mtil_dag", "bqcdg_mtdagmt", "bqcdg_w_mult", "bqcdg_w_mult_dag",
+                  "bqcdg_w_dagger_w"):
+            getattr(L, n).argtypes = [vp, dp, dp, P(Params)]
+        L.bqcdg_cg.argtypes = [vp, dp, dp, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
+        L.bqcdg_quda_solver.argtypes = [vp, dp, dp, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
+        L.bqcdg_solve.argtypes = [vp, dp, dp, P(Params), P(SolverOpts), P(SolveInfo)]
+        L.bqcdg_solver_opts_default.argtypes = [P(SolverOpts)]
+        L.bqcdg_solver_opts_default.restype = None
+        L.bqcdg_dsf.argtypes = [vp, dp, C.c_double, P(Params), dp, dp]
+        L.bqcdg_clover_dsf.argtypes = [vp, i, dp, dp, dp, C.c_double]
+        L.bqcdg_clover_dsd.argtypes = [vp, i, dp, C.c_double]
+        L.bqcdg_field_create.argtypes = [vp, P(C.c_int)]
+        L.bqcdg_field_upload.argtypes = [vp, i, dp]
+        L.bqcdg_field_download.argtypes = [vp, i, dp]
+        L.bqcdg_field_destroy.argtypes = [vp, i]
+        L.bqcdg_solve_dev.argtypes = [vp, i, i, P(Params), P(SolverOpts), P(SolveInfo)]
+        L.bqcdg_mdagm_dev.argtypes = [vp, i, i, P(Params), i, i, P(C.c_double)]
+        L.bqcdg_time_pass.argtypes = [vp, i, P(Params), i, i, P(C.c_double)]
+        L.bqcdg_ranset.argtypes = [vp, C.c_longlong, C.c_longlong]
+        L.bqcdg_ranget.argtypes = [vp, P(C.c_longlong)]
+        L.bqcdg_conf_hot.argtypes = [vp]
+        L.bqcdg_conf_cold.argtypes = [vp]
+        L.bqcdg_conf_relax.argtypes = [vp, i]
+        L.bqcdg_sg.argtypes = [vp, P(C.c_double)]
+        L.bqcdg_field_gauss.argtypes = [vp, i, C.c_double]
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    return _lib_handle()
+
+
+def _ptr(a, dtype):
+    if a is None:
+        return None
+    if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous):
+        raise TypeError("expected a C-contiguous %s array" % np.dtype(dtype).name)
+    return a.ctypes.data
+
+
+def _check(status, what):
+    if status != OK:
+        raise BqcdgError(status, what)
+
+
+@dataclass
+class HmcPara:
+    """The hot-path part of type(hmc_para) (modules/typedef_hmc.F90:32-44)."""
+    kappa: float
+    csw: float = 0.0
+    h: float = 0.0
+    rho: float = 0.0
+
+    @property
+    def csw_kappa(self):
+        return self.csw * self.kappa  # bqcd.F90:170
+
+    def params(self, rho=None):
+        return Params(self.kappa, self.csw_kappa, self.h, self.rho if rho is None else rho)
+
+
+class Lattice:
+    """One GPU context over a whole single-process lattice."""
+
+    def __init__(self, L, bc=(1, 1, 1, -1), device=0):
+        self.L = tuple(int(x) for x in L)
+        self.bc = tuple(int(x) for x in bc)
+        h = C.c_void_p()
+        _check(lib().bqcdg_create(C.byref(h), (C.c_int * 4)(*self.L), (C.c_int * 4)(*self.bc), device),
+               "bqcdg_create")
+        self.h = h
+        self.volh = lib().bqcdg_volh(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().bqcdg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def device_bytes(self):
+        return lib().bqcdg_device_bytes(self.h)
+
+    # ---- fields ----
+    def spinor(self):
+        return np.zeros((self.volh, 3, 4), np.complex128)
+
+    def load_gauge(self, u, flipped):
+        _check(lib().bqcdg_load_gauge(self.h, _ptr(u, np.complex128), int(flipped)), "load_gauge")
+
+    def get_gauge(self, flipped=False):
+        u = np.zeros((4, 2, self.volh, 3, 3), np.complex128)
+        _check(lib().bqcdg_get_gauge(self.h, u.ctypes.data, int(flipped)), "get_gauge")
+        return u
+
+    def load_clover(self, a=None, ainv=None, b=None):
+        _check(lib().bqcdg_load_clover(self.h, _ptr(a, np.complex128), _ptr(ainv, np.complex128),
+                                       _ptr(b, np.complex128)), "load_clover")
+
+    def clover_init(self, csw_kappa):
+        """clover_init(a, i, b, u, csw_kappa) on the device from the loaded links."""
+        _check(lib().bqcdg_clover_init(self.h, csw_kappa), "clover_init")
+
+    def get_clover(self):
+        out = [np.zeros((2, self.volh, 2, 18), np.complex128) for _ in range(3)]
+        _check(lib().bqcdg_get_clover(self.h, *[o.ctypes.data for o in out]), "get_clover")
+        return tuple(out)
+
+    def clover_action(self, eo=ODD):
+        v = C.c_double()
+        _check(lib().bqcdg_clover_action(self.h, eo, C.byref(v)), "clover_action")
+        return v.value
+
+    # ---- operators (reference names) ----
+    def d(self, e, o, inp):
+        out = self.spinor()
+        _check(lib().bqcdg_d(self.h, e, o, out.ctypes.data, _ptr(inp, np.complex128)), "d")
+        return out
+
+    def d_dag(self, e, o, inp):
+        out = self.spinor()
+        _check(lib().bqcdg_d_dag(self.h, e, o, out.ctypes.data, _ptr(inp, np.complex128)), "d_dag")
+        return out
+
+    def clover_mult_a(self, eo, inp):
+        out = self.spinor()
+        _check(lib().bqcdg_clover_mult_a(self.h, eo, out.ctypes.data, _ptr(inp, np.complex128)), "clover_mult_a")
+        return out
+
+    def clover_mult_ao(self, eo, x):
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        _check(lib().bqcdg_clover_mult_ao(self.h, eo, x.ctypes.data), "clover_mult_ao")
+        return x
+
+    def clover_mult_b(self, eo, x):
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        _check(lib().bqcdg_clover_mult_b(self.h, eo, x.ctypes.data), "clover_mult_b")
+        return x
+
+    def _op(self, name, inp, para):
+        out = self.spinor()
+        prm = para.params() if isinstance(para, HmcPara) else para
+        _check(getattr(lib(), "bqcdg_" + name)(self.h, out.ctypes.data, _ptr(inp, np.complex128), C.byref(prm)),
+               name)
+        return out
+
+    def mtil(self, inp, para):
+        return self._op("mtil", inp, para)
+
+    def mtil_dag(self, inp, para):
+        return self._op("mtil_dag", inp, para)
+
+    def mtdagmt(self, inp, para):
+        return self._op("mtdagmt", inp, para)
+
+    def w_mult(self, inp, para):
+        return self._op("w_mult", inp, para)
+
+    def w_mult_dag(self, inp, para):
+        return self._op("w_mult_dag", inp, para)
+
+    def w_dagger_w(self, inp, para):
+        return self._op("w_dagger_w", inp, para)
+
+    # ---- solvers ----
+    def cg(self, x, b, para, rest, maxiter=1000, log=0, rho=None):
+        """cg(w_dagger_w or mtdagmt, x, b, ...) (cg.F90:51): x is the initial
+        guess; returns (x, iterations, info).  Raises on no convergence unless
+        log == 2 (then info.converged is 0)."""
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        it = C.c_int()
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        cp = CgPara(rest, maxiter, log)
+        _check(lib().bqcdg_cg(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(cp),
+                              C.byref(it), C.byref(info)), "cg")
+        return x, it.value, info
+
+    def quda_solver(self, x, b, para, rest, maxiter=1000, log=0, rho=None):
+        """quda_solver(matrix_mult, x, b, para, conf, iterations, rho)
+        (invert_quda.F90:96): mixed precision, absolute stop, true residual
+        re-checked in FP64."""
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        it = C.c_int()
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        cp = CgPara(rest, maxiter, log)
+        _check(lib().bqcdg_quda_solver(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(cp),
+                                       C.byref(it), C.byref(info)), "quda_solver")
+        return x, it.value, info
+
+    def solve(self, x, b, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000, delta=0.1,
+              time_kernels=False, rho=None):
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, int(time_kernels))
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        st = lib().bqcdg_solve(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(o),
+                               C.byref(info))
+        if st not in (OK, ENOCONV):
+            _check(st, "solve")
+        return x, info
+
+    # ---- forces ----
+    def dsf(self, p, step, para, a, b):
+        """dsf(p, conf, step, para, a, b) (dsf.F90:28); p is updated in place."""
+        prm = para.params() if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_dsf(self.h, _ptr(p, np.float64), step, C.byref(prm), _ptr(a, np.complex128),
+                               _ptr(b, np.complex128)), "dsf")
+        return p
+
+    def clover_dsf(self, eo, p, b, a, s):
+        _check(lib().bqcdg_clover_dsf(self.h, eo, _ptr(p, np.float64), _ptr(b, np.complex128),
+                                      _ptr(a, np.complex128), s), "clover_dsf")
+        return p
+
+    def clover_dsd(self, eo, p, s):
+        _check(lib().bqcdg_clover_dsd(self.h, eo, _ptr(p, np.float64), s), "clover_dsd")
+        return p
+
+    # ---- seeded inputs on the device (ranf.F90, ran.F90, conf.F90, cooling.F90) ----
+    def ranset(self, seed, skip=0):
+        _check(lib().bqcdg_ranset(self.h, seed, skip), "ranset")
+
+    def ranget(self):
+        s = C.c_longlong()
+        _check(lib().bqcdg_ranget(self.h, C.byref(s)), "ranget")
+        return s.value
+
+    def conf_hot(self):
+        _check(lib().bqcdg_conf_hot(self.h), "conf_hot")
+
+    def conf_cold(self):
+        _check(lib().bqcdg_conf_cold(self.h), "conf_cold")
+
+    def conf_relax(self, n=1):
+        _check(lib().bqcdg_conf_relax(self.h, n), "conf_relax")
+
+    def sg(self):
+        v = C.c_double()
+        _check(lib().bqcdg_sg(self.h, C.byref(v)), "sg")
+        return v.value
+
+    def plaq_energy(self):
+        """sg / (6 V) as BQCD prints it (mc.F90:63)."""
+        return self.sg() / (6.0 * 2 * self.volh)
+
+    def field_gauss(self, handle, var=0.5):
+        _check(lib().bqcdg_field_gauss(self.h, handle, var), "field_gauss")
+
+    # ---- resident fields ----
+    def field(self, host=None):
+        h = C.c_int()
+        _check(lib().bqcdg_field_create(self.h, C.byref(h)), "field_create")
+        if host is not None:
+            _check(lib().bqcdg_field_upload(self.h, h.value, _ptr(host, np.complex128)), "field_upload")
+        return h.value
+
+    def field_get(self, handle):
+        out = self.spinor()
+        _check(lib().bqcdg_field_download(self.h, handle, out.ctypes.data), "field_download")
+        return out
+
+    def field_set(self, handle, host):
+        _check(lib().bqcdg_field_upload(self.h, handle, _ptr(host, np.complex128)), "field_upload")
+
+    def solve_dev(self, hx, hb, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000, delta=0.1,
+                  time_kernels=False, rho=None):
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, int(time_kernels))
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        st = lib().bqcdg_solve_dev(self.h, hx, hb, C.byref(prm), C.byref(o), C.byref(info))
+        if st not in (OK, ENOCONV):
+            _check(st, "solve_dev")
+        return info
+
+    def mdagm_dev(self, hout, hin, para, precision, n, rho=None):
+        ms = C.c_double()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_mdagm_dev(self.h, hout, hin, C.byref(prm), precision, n, C.byref(ms)), "mdagm_dev")
+        return ms.value
+
+    def time_pass(self, hin, para, precision, n, rho=None):
+        ms = C.c_double()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_time_pass(self.h, hin, C.byref(prm), precision, n, C.byref(ms)), "time_pass")
+        return ms.value

@@ -1,0 +1,707 @@
+// bqcdg_internal.cuh -- device data layouts and the shared Wilson-clover
+// arithmetic of the B200 (sm_100a) implementation of BQCD's fermion hot path.
+//
+// Host-facing arrays use BQCD's Fortran layouts (defs.h:64-78); on the device
+// every field is component-major ("structure of arrays") so that one warp
+// reading one component of 32 consecutive sites issues one contiguous 512-byte
+// (FP64) transaction:
+//
+//   spinor  F64 : double2 [12][stride]      component k = colour*4 + spin
+//           F32 : float4  [6][stride]       two components per float4
+//           F16 : int4    [3][stride]       eight int16 components per int4,
+//                 + float norm[stride]      value = q * norm / 32767
+//   link    F64 : double2 [9][stride]       18-real, k = col*3 + row
+//           F32 : float4  [3][stride]       12-real: columns 1,2 (third column
+//           F16 : short4  [3][stride]       rebuilt as in su3.F90:300-310)
+//   clover  F64 : double2 [36][stride]      per parity: chiral block chi*18 +
+//           F32 : float4  [18][stride]      the 18-slot packing of clover.h:28-82
+//           F16 : int4    [9][stride] + float norm[stride]
+//
+// Device links are always stored periodic (unflipped); the fermion boundary
+// sign of flip_bc.F90:97-121 is applied inside the stencil kernels, so the
+// operators act exactly like BQCD's on links bracketed by flip_bc().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace bqcdg {
+
+enum class Prec : int { F64 = 0, F32 = 1, F16 = 2 };
+
+// ---------------------------------------------------------------------------
+// complex arithmetic
+// ---------------------------------------------------------------------------
+template <typename R>
+struct cx {
+  R x, y;
+};
+template <typename R>
+__device__ __forceinline__ cx<R> mkc(R a, R b) { return cx<R>{a, b}; }
+template <typename R>
+__device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename R>
+__device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) { return {a.x - b.x, a.y - b.y}; }
+template <typename R>
+__device__ __forceinline__ cx<R> operator-(cx<R> a) { return {-a.x, -a.y}; }
+template <typename R>
+__device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename R>
+__device__ __forceinline__ cx<R> operator*(R s, cx<R> a) { return {s * a.x, s * a.y}; }
+template <typename R>
+__device__ __forceinline__ cx<R> conjg(cx<R> a) { return {a.x, -a.y}; }
+// i * a
+template <typename R>
+__device__ __forceinline__ cx<R> itimes(cx<R> a) { return {-a.y, a.x}; }
+// a * conj(b)
+template <typename R>
+__device__ __forceinline__ cx<R> mulc(cx<R> a, cx<R> b) {
+  return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+// acc + a*b
+template <typename R>
+__device__ __forceinline__ cx<R> fma_c(cx<R> acc, cx<R> a, cx<R> b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+// acc + conj(a)*b
+template <typename R>
+__device__ __forceinline__ cx<R> fma_cc(cx<R> acc, cx<R> a, cx<R> b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+  return acc;
+}
+template <typename R>
+__device__ __forceinline__ R norm2(cx<R> a) { return a.x * a.x + a.y * a.y; }
+
+template <typename R>
+struct Spinor {
+  cx<R> c[4][3];  // [spin][colour]
+};
+template <typename R>
+struct Half {
+  cx<R> c[2][3];
+};
+template <typename R>
+struct Link {
+  cx<R> m[3][3];  // [row][col]
+};
+
+template <typename R>
+__device__ __forceinline__ void zero(Spinor<R>& s) {
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) s.c[a][b] = mkc<R>(0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// geometry: even/odd index i = ilex/2 (index.F90:58-76), parity (x+y+z+t)%2
+// ---------------------------------------------------------------------------
+struct Geom {
+  int L[4];
+  int Lxh;
+  int volh;
+  int stride;      // padded per-component stride of every field
+  int bcsign[4];   // fermion boundary sign per direction (+1 / -1)
+};
+
+struct Site {
+  int x[4];
+  int base;  // i - x/2 : index offset of the (y,z,t) row
+};
+
+__device__ __forceinline__ Site site_coords(const Geom& g, int i, int parity) {
+  Site s;
+  int xh = i % g.Lxh;
+  int r = i / g.Lxh;
+  s.x[1] = r % g.L[1];
+  r /= g.L[1];
+  s.x[2] = r % g.L[2];
+  s.x[3] = r / g.L[2];
+  s.x[0] = 2 * xh + ((s.x[1] + s.x[2] + s.x[3] + parity) & 1);
+  s.base = i - xh;
+  return s;
+}
+
+// index of the neighbour of site s in direction mu (fwd: +1, bwd: -1)
+__device__ __forceinline__ int neighbour(const Geom& g, const Site& s, int i, int mu, bool fwd) {
+  if (mu == 0) {
+    int x = s.x[0] + (fwd ? 1 : -1);
+    if (x < 0) x += g.L[0];
+    if (x >= g.L[0]) x -= g.L[0];
+    return s.base + (x >> 1);
+  }
+  int step = g.Lxh;
+  if (mu >= 2) step *= g.L[1];
+  if (mu == 3) step *= g.L[2];
+  if (fwd) return s.x[mu] == g.L[mu] - 1 ? i - (g.L[mu] - 1) * step : i + step;
+  return s.x[mu] == 0 ? i + (g.L[mu] - 1) * step : i - step;
+}
+
+// boundary sign of the link used by a hop: the forward hop uses U_mu(x), the
+// backward hop U_mu(x-mu); flip_bc negates links on the slice x_mu = L_mu-1.
+__device__ __forceinline__ int hop_sign(const Geom& g, const Site& s, int mu, bool fwd) {
+  if (g.bcsign[mu] > 0) return 1;
+  return (fwd ? s.x[mu] == g.L[mu] - 1 : s.x[mu] == 0) ? g.bcsign[mu] : 1;
+}
+
+// ---------------------------------------------------------------------------
+// field views
+// ---------------------------------------------------------------------------
+template <Prec P>
+struct SpinorView;
+
+template <>
+struct SpinorView<Prec::F64> {
+  using R = double;
+  double2* v;
+  int stride;
+  __device__ __forceinline__ void load(int i, Spinor<double>& s) const {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        double2 t = __ldg(v + (c * 4 + sp) * stride + i);
+        s.c[sp][c] = mkc(t.x, t.y);
+      }
+  }
+  // spins (s0, s0+1) only
+  __device__ __forceinline__ void load_pair(int i, int s0, cx<double> h[2][3]) const {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        double2 t = __ldg(v + (c * 4 + s0 + k) * stride + i);
+        h[k][c] = mkc(t.x, t.y);
+      }
+  }
+  __device__ __forceinline__ void store(int i, const Spinor<double>& s) const {
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) v[(c * 4 + sp) * stride + i] = make_double2(s.c[sp][c].x, s.c[sp][c].y);
+  }
+};
+
+template <>
+struct SpinorView<Prec::F32> {
+  using R = float;
+  float4* v;
+  int stride;
+  __device__ __forceinline__ void load(int i, Spinor<float>& s) const {
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      float4 t = __ldg(v + k * stride + i);
+      int k0 = 2 * k, k1 = 2 * k + 1;
+      s.c[k0 & 3][k0 >> 2] = mkc(t.x, t.y);
+      s.c[k1 & 3][k1 >> 2] = mkc(t.z, t.w);
+    }
+  }
+  __device__ __forceinline__ void load_pair(int i, int s0, cx<float> h[2][3]) const {
+    // components (c*4+s0, c*4+s0+1) sit in float4 number c*2 + s0/2
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float4 t = __ldg(v + (c * 2 + (s0 >> 1)) * stride + i);
+      h[0][c] = mkc(t.x, t.y);
+      h[1][c] = mkc(t.z, t.w);
+    }
+  }
+  __device__ __forceinline__ void store(int i, const Spinor<float>& s) const {
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      int k0 = 2 * k, k1 = 2 * k + 1;
+      v[k * stride + i] = make_float4(s.c[k0 & 3][k0 >> 2].x, s.c[k0 & 3][k0 >> 2].y, s.c[k1 & 3][k1 >> 2].x,
+                                      s.c[k1 & 3][k1 >> 2].y);
+    }
+  }
+};
+
+__device__ __forceinline__ float q2f(short q, float scale) { return (float)q * scale; }
+__device__ __forceinline__ short f2q(float v, float inv) {
+  return (short)__float2int_rn(v * inv);
+}
+
+template <>
+struct SpinorView<Prec::F16> {
+  using R = float;
+  int4* v;      // [3][stride], each int4 = 8 int16 = 4 complex
+  float* norm;  // [stride]
+  int stride;
+  __device__ __forceinline__ void load(int i, Spinor<float>& s) const {
+    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      int4 t = __ldg(v + k * stride + i);
+      const short* q = reinterpret_cast<const short*>(&t);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        int comp = 4 * k + j;  // colour k, spin j
+        s.c[comp & 3][comp >> 2] = mkc(q2f(q[2 * j], scale), q2f(q[2 * j + 1], scale));
+      }
+    }
+  }
+  __device__ __forceinline__ void load_pair(int i, int s0, cx<float> h[2][3]) const {
+    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      // colour c occupies int4 number c; spins s0,s0+1 are its halves
+      const int2* p = reinterpret_cast<const int2*>(v + c * stride + i);
+      int2 t = __ldg(p + (s0 >> 1));
+      const short* q = reinterpret_cast<const short*>(&t);
+      h[0][c] = mkc(q2f(q[0], scale), q2f(q[1], scale));
+      h[1][c] = mkc(q2f(q[2], scale), q2f(q[3], scale));
+    }
+  }
+  __device__ __forceinline__ void store(int i, const Spinor<float>& s) const {
+    float m = 0.f;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) m = fmaxf(m, fmaxf(fabsf(s.c[a][b].x), fabsf(s.c[a][b].y)));
+    float inv = m > 0.f ? 32767.0f / m : 0.f;
+    norm[i] = m;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      short q[8];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        q[2 * j] = f2q(s.c[j][k].x, inv);
+        q[2 * j + 1] = f2q(s.c[j][k].y, inv);
+      }
+      v[k * stride + i] = *reinterpret_cast<int4*>(q);
+    }
+  }
+};
+
+// links --------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void reconstruct_col3(Link<R>& u) {
+  // su3.F90:300-310: third column from the first two
+  u.m[0][2] = conjg(u.m[1][0] * u.m[2][1] - u.m[2][0] * u.m[1][1]);
+  u.m[1][2] = conjg(u.m[2][0] * u.m[0][1] - u.m[0][0] * u.m[2][1]);
+  u.m[2][2] = conjg(u.m[0][0] * u.m[1][1] - u.m[1][0] * u.m[0][1]);
+}
+
+template <Prec P>
+struct GaugeView;
+
+template <>
+struct GaugeView<Prec::F64> {
+  using R = double;
+  double2* v;  // [4][2][9][stride]
+  int stride;
+  __device__ __forceinline__ void load(int mu, int eo, int i, Link<double>& u) const {
+    const double2* b = v + (size_t)((mu * 2 + eo) * 9) * stride + i;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        double2 t = __ldg(b + (c * 3 + r) * stride);
+        u.m[r][c] = mkc(t.x, t.y);
+      }
+  }
+};
+
+template <>
+struct GaugeView<Prec::F32> {
+  using R = float;
+  float4* v;  // [4][2][3][stride]
+  int stride;
+  __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
+    const float4* b = v + (size_t)((mu * 2 + eo) * 3) * stride + i;
+    float4 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
+    u.m[0][0] = mkc(t0.x, t0.y);
+    u.m[1][0] = mkc(t0.z, t0.w);
+    u.m[2][0] = mkc(t1.x, t1.y);
+    u.m[0][1] = mkc(t1.z, t1.w);
+    u.m[1][1] = mkc(t2.x, t2.y);
+    u.m[2][1] = mkc(t2.z, t2.w);
+    reconstruct_col3(u);
+  }
+};
+
+template <>
+struct GaugeView<Prec::F16> {
+  using R = float;
+  short4* v;  // [4][2][3][stride], entries scaled by 32767
+  int stride;
+  __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
+    const short4* b = v + (size_t)((mu * 2 + eo) * 3) * stride + i;
+    const float sc = 1.0f / 32767.0f;
+    short4 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
+    u.m[0][0] = mkc(t0.x * sc, t0.y * sc);
+    u.m[1][0] = mkc(t0.z * sc, t0.w * sc);
+    u.m[2][0] = mkc(t1.x * sc, t1.y * sc);
+    u.m[0][1] = mkc(t1.z * sc, t1.w * sc);
+    u.m[1][1] = mkc(t2.x * sc, t2.y * sc);
+    u.m[2][1] = mkc(t2.z * sc, t2.w * sc);
+    reconstruct_col3(u);
+  }
+};
+
+// clover blocks ------------------------------------------------------------
+// Packed 18-slot chiral block (clover.h:28-55): slot 0 = (A11,A22), 10 =
+// (A33,A44), 16 = (A55,A66) real diagonals; upper entries in slots 1-9,11-15,17.
+
+template <Prec P>
+struct CloverView;
+
+template <>
+struct CloverView<Prec::F64> {
+  using R = double;
+  double2* v;  // [36][stride] for one parity
+  int stride;
+  __device__ __forceinline__ void load_block(int i, int chi, cx<double> a[18]) const {
+#pragma unroll
+    for (int k = 0; k < 18; k++) {
+      double2 t = __ldg(v + (chi * 18 + k) * stride + i);
+      a[k] = mkc(t.x, t.y);
+    }
+  }
+};
+
+template <>
+struct CloverView<Prec::F32> {
+  using R = float;
+  float4* v;  // [18][stride]
+  int stride;
+  __device__ __forceinline__ void load_block(int i, int chi, cx<float> a[18]) const {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float4 t = __ldg(v + (chi * 9 + k) * stride + i);
+      a[2 * k] = mkc(t.x, t.y);
+      a[2 * k + 1] = mkc(t.z, t.w);
+    }
+  }
+};
+
+template <>
+struct CloverView<Prec::F16> {
+  using R = float;
+  int4* v;  // [9][stride], 8 int16 = 4 slots each
+  float* norm;
+  int stride;
+  __device__ __forceinline__ void load_block(int i, int chi, cx<float> a[18]) const {
+    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
+    // slots chi*18 .. chi*18+17 live in int4 numbers (chi*18)/4 .. (chi*18+17)/4
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      int word = chi * 4 + k;  // block 0: words 0-4, block 1: words 4-8
+      int4 t = __ldg(v + word * stride + i);
+      const short* q = reinterpret_cast<const short*>(&t);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        int slot = 4 * word + j - chi * 18;
+        if (slot >= 0 && slot < 18) a[slot] = mkc(q[2 * j] * scale, q[2 * j + 1] * scale);
+      }
+    }
+  }
+};
+
+// y = A x for one packed Hermitian 6x6 block (clover_mult_a.h90)
+template <typename R>
+__device__ __forceinline__ void clover_block_mv(const cx<R>* a, const cx<R> x[6], cx<R> y[6]) {
+  const R d0 = a[0].x, d1 = a[0].y, d2 = a[10].x, d3 = a[10].y, d4 = a[16].x, d5 = a[16].y;
+  // upper-triangle slots
+  const cx<R> a01 = a[1], a02 = a[2], a03 = a[3], a04 = a[4], a05 = a[5];
+  const cx<R> a12 = a[6], a13 = a[7], a14 = a[8], a15 = a[9];
+  const cx<R> a23 = a[11], a24 = a[12], a25 = a[13];
+  const cx<R> a34 = a[14], a35 = a[15];
+  const cx<R> a45 = a[17];
+  cx<R> t;
+  t = d0 * x[0];
+  t = fma_c(t, a01, x[1]); t = fma_c(t, a02, x[2]); t = fma_c(t, a03, x[3]); t = fma_c(t, a04, x[4]); t = fma_c(t, a05, x[5]);
+  y[0] = t;
+  t = d1 * x[1];
+  t = fma_cc(t, a01, x[0]); t = fma_c(t, a12, x[2]); t = fma_c(t, a13, x[3]); t = fma_c(t, a14, x[4]); t = fma_c(t, a15, x[5]);
+  y[1] = t;
+  t = d2 * x[2];
+  t = fma_cc(t, a02, x[0]); t = fma_cc(t, a12, x[1]); t = fma_c(t, a23, x[3]); t = fma_c(t, a24, x[4]); t = fma_c(t, a25, x[5]);
+  y[2] = t;
+  t = d3 * x[3];
+  t = fma_cc(t, a03, x[0]); t = fma_cc(t, a13, x[1]); t = fma_cc(t, a23, x[2]); t = fma_c(t, a34, x[4]); t = fma_c(t, a35, x[5]);
+  y[3] = t;
+  t = d4 * x[4];
+  t = fma_cc(t, a04, x[0]); t = fma_cc(t, a14, x[1]); t = fma_cc(t, a24, x[2]); t = fma_cc(t, a34, x[3]); t = fma_c(t, a45, x[5]);
+  y[4] = t;
+  t = d5 * x[5];
+  t = fma_cc(t, a05, x[0]); t = fma_cc(t, a15, x[1]); t = fma_cc(t, a25, x[2]); t = fma_cc(t, a35, x[3]); t = fma_cc(t, a45, x[4]);
+  y[5] = t;
+}
+
+// out = A in on one site, both chiral blocks (clover_mult_a.F90:45-95): the
+// blocks act on x+- = psi(spin 1,2) +- psi(spin 3,4).
+template <Prec P, typename R>
+__device__ __forceinline__ void clover_apply(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out) {
+  cx<R> x[6], y[6], a[18];
+#pragma unroll
+  for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3];
+  A.load_block(i, 0, a);
+  clover_block_mv(a, x, y);
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    out.c[k / 3][k % 3] = y[k];
+    out.c[k / 3 + 2][k % 3] = y[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] - in.c[k / 3 + 2][k % 3];
+  A.load_block(i, 1, a);
+  clover_block_mv(a, x, y);
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    out.c[k / 3][k % 3] = out.c[k / 3][k % 3] + y[k];
+    out.c[k / 3 + 2][k % 3] = out.c[k / 3 + 2][k % 3] - y[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wilson hop (d/D21.F90, d/D21xyzt.F90).  Forward hop: (1 - s gamma_mu)
+// projection of psi(x+mu), times U_mu(x); backward hop: (1 + s gamma_mu)
+// projection of psi(x-mu) times U_mu(x-mu)^+; s = +1 for d, -1 for d_dag.
+// gamma basis of BQCD (UKQCD / Dirac): gamma_4 = diag(1,1,-1,-1).
+// ---------------------------------------------------------------------------
+template <typename R, bool DAG>
+__device__ __forceinline__ void project(const Spinor<R>& p, int mu, bool fwd, cx<R> h[2][3]) {
+  const R s = DAG ? R(-1) : R(1);
+  const R sg = fwd ? -s : s;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 0) {
+      h[0][c] = p.c[0][c] + sg * itimes(p.c[3][c]);
+      h[1][c] = p.c[1][c] + sg * itimes(p.c[2][c]);
+    } else if (mu == 1) {
+      h[0][c] = p.c[0][c] + sg * p.c[3][c];
+      h[1][c] = p.c[1][c] - sg * p.c[2][c];
+    } else {
+      h[0][c] = p.c[0][c] + sg * itimes(p.c[2][c]);
+      h[1][c] = p.c[1][c] - sg * itimes(p.c[3][c]);
+    }
+  }
+}
+
+// b += reconstruction of the transported forward half spinor f
+template <typename R, bool DAG>
+__device__ __forceinline__ void recon_fwd(Spinor<R>& b, int mu, const cx<R> f[2][3]) {
+  const R s = DAG ? R(-1) : R(1);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 3) {
+      if (!DAG) {
+        b.c[2][c] = b.c[2][c] + R(2) * f[0][c];
+        b.c[3][c] = b.c[3][c] + R(2) * f[1][c];
+      } else {
+        b.c[0][c] = b.c[0][c] + R(2) * f[0][c];
+        b.c[1][c] = b.c[1][c] + R(2) * f[1][c];
+      }
+    } else {
+      b.c[0][c] = b.c[0][c] + f[0][c];
+      b.c[1][c] = b.c[1][c] + f[1][c];
+      if (mu == 0) {
+        b.c[2][c] = b.c[2][c] + s * itimes(f[1][c]);
+        b.c[3][c] = b.c[3][c] + s * itimes(f[0][c]);
+      } else if (mu == 1) {
+        b.c[2][c] = b.c[2][c] + s * f[1][c];
+        b.c[3][c] = b.c[3][c] - s * f[0][c];
+      } else {
+        b.c[2][c] = b.c[2][c] + s * itimes(f[0][c]);
+        b.c[3][c] = b.c[3][c] - s * itimes(f[1][c]);
+      }
+    }
+  }
+}
+
+template <typename R, bool DAG>
+__device__ __forceinline__ void recon_bwd(Spinor<R>& b, int mu, const cx<R> f[2][3]) {
+  const R s = DAG ? R(-1) : R(1);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 3) {
+      if (!DAG) {
+        b.c[0][c] = b.c[0][c] + R(2) * f[0][c];
+        b.c[1][c] = b.c[1][c] + R(2) * f[1][c];
+      } else {
+        b.c[2][c] = b.c[2][c] + R(2) * f[0][c];
+        b.c[3][c] = b.c[3][c] + R(2) * f[1][c];
+      }
+    } else {
+      b.c[0][c] = b.c[0][c] + f[0][c];
+      b.c[1][c] = b.c[1][c] + f[1][c];
+      if (mu == 0) {
+        b.c[2][c] = b.c[2][c] - s * itimes(f[1][c]);
+        b.c[3][c] = b.c[3][c] - s * itimes(f[0][c]);
+      } else if (mu == 1) {
+        b.c[2][c] = b.c[2][c] - s * f[1][c];
+        b.c[3][c] = b.c[3][c] + s * f[0][c];
+      } else {
+        b.c[2][c] = b.c[2][c] - s * itimes(f[0][c]);
+        b.c[3][c] = b.c[3][c] + s * itimes(f[1][c]);
+      }
+    }
+  }
+}
+
+// f = sgn * U h   (colour vectors h[0], h[1])
+template <typename R>
+__device__ __forceinline__ void mul_u(const Link<R>& u, const cx<R> h[2][3], R sgn, cx<R> f[2][3]) {
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      cx<R> t = u.m[r][0] * h[k][0];
+      t = fma_c(t, u.m[r][1], h[k][1]);
+      t = fma_c(t, u.m[r][2], h[k][2]);
+      f[k][r] = sgn * t;
+    }
+}
+// f = sgn * U^+ h
+template <typename R>
+__device__ __forceinline__ void mul_ud(const Link<R>& u, const cx<R> h[2][3], R sgn, cx<R> f[2][3]) {
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      cx<R> t = mkc<R>(0, 0);
+      t = fma_cc(t, u.m[0][r], h[k][0]);
+      t = fma_cc(t, u.m[1][r], h[k][1]);
+      t = fma_cc(t, u.m[2][r], h[k][2]);
+      f[k][r] = sgn * t;
+    }
+}
+
+// b = sum over the 8 hops of the even/odd hopping term: out(parity e, site i)
+// from the field ``in`` of the opposite parity (d/D21.F90:29-77).
+template <Prec PS, Prec PG, bool DAG>
+__device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Site& st,
+                                           const SpinorView<PS>& in, const GaugeView<PG>& U,
+                                           Spinor<typename SpinorView<PS>::R>& b) {
+  using R = typename SpinorView<PS>::R;
+  const int o = 1 - e;
+  zero(b);
+#pragma unroll
+  for (int mu = 3; mu >= 0; mu--) {
+    // forward hop
+    {
+      int j = neighbour(g, st, i, mu, true);
+      cx<R> h[2][3], f[2][3];
+      if (mu == 3) {
+        // (1 -+ gamma_4) keeps two spins: (3,4) for d, (1,2) for d_dag
+        in.load_pair(j, DAG ? 0 : 2, h);
+      } else {
+        Spinor<R> p;
+        in.load(j, p);
+        project<R, DAG>(p, mu, true, h);
+      }
+      Link<R> u;
+      U.load(mu, e, i, u);
+      mul_u(u, h, (R)hop_sign(g, st, mu, true), f);
+      recon_fwd<R, DAG>(b, mu, f);
+    }
+    // backward hop
+    {
+      int j = neighbour(g, st, i, mu, false);
+      cx<R> h[2][3], f[2][3];
+      if (mu == 3) {
+        in.load_pair(j, DAG ? 2 : 0, h);
+      } else {
+        Spinor<R> p;
+        in.load(j, p);
+        project<R, DAG>(p, mu, false, h);
+      }
+      Link<R> u;
+      U.load(mu, o, j, u);
+      mul_ud(u, h, (R)hop_sign(g, st, mu, false), f);
+      recon_bwd<R, DAG>(b, mu, f);
+    }
+  }
+}
+
+// (1 + i h gamma_5) x, gamma_5 swapping spins 1<->3, 2<->4 (h_mult.F90:51-82)
+template <typename R>
+__device__ __forceinline__ void h_mult_b(Spinor<R>& x, R h) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    cx<R> x1 = x.c[0][c], x2 = x.c[1][c], x3 = x.c[2][c], x4 = x.c[3][c];
+    x.c[0][c] = x1 + h * itimes(x3);
+    x.c[1][c] = x2 + h * itimes(x4);
+    x.c[2][c] = x3 + h * itimes(x1);
+    x.c[3][c] = x4 + h * itimes(x2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// deterministic block reductions
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void block_reduce_store(double (&v)[N], double* partial, int nblocks_stride) {
+  __shared__ double red[N][32];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    double x = v[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    v[k] = x;
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) red[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      double x = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+      if (lane == 0) partial[k * nblocks_stride + blockIdx.x] = x;
+    }
+  }
+}
+
+// Called by every block after block_reduce_store; returns true in thread 0 of
+// the last block to arrive, which then sums the partials in block order.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+  __shared__ bool is_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return is_last;
+}
+
+template <int N>
+__device__ __forceinline__ void final_sum(const double* partial, int nblocks_stride, double (&out)[N]) {
+  // executed by the whole last block: warp-parallel fixed-order sum
+  __shared__ double red[N][32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    double x = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) x += __ldcg(partial + k * nblocks_stride + b);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) red[k][warp] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    double x = 0.0;
+    for (int w = 0; w < nw; w++) x += red[k][w];
+    out[k] = x;
+  }
+  __syncthreads();
+}
+
+}  // namespace bqcdg

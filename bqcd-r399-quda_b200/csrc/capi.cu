@@ -1,0 +1,1090 @@
+// capi.cu -- host runtime and C ABI (include/bqcdg.h).
+//
+// A context owns one CUDA stream, the resident FP64 gauge and clover fields
+// (plus their reduced-precision copies, rebuilt lazily after each reload),
+// scratch spinors and the reduction buffers.  Host arrays in BQCD's Fortran
+// layouts are staged with one contiguous copy and converted on the device.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../../include/bqcdg.h"
+#include "kernels.cuh"
+
+using namespace bqcdg;
+
+namespace {
+
+struct Spin64 {
+  double2* v = nullptr;
+};
+
+int status_from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return BQCDG_OK;
+  if (e == cudaErrorMemoryAllocation) return BQCDG_ENOMEM;
+  return BQCDG_ECUDA;
+}
+
+}  // namespace
+
+struct bqcdg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Geom g{};
+  long long bytes = 0;
+  std::vector<void*> allocations;
+
+  double2* staging = nullptr;  // Fortran-layout staging (largest field: gauge)
+  size_t staging_bytes = 0;
+
+  double2* gauge64 = nullptr;
+  bool have_gauge = false;
+  bool gauge_su3 = false;
+  void* gauge_s[3] = {nullptr, nullptr, nullptr};  // by Prec
+  bool gauge_s_ok[3] = {false, false, false};
+
+  double2* A[2] = {nullptr, nullptr};
+  double2* Ainv[2] = {nullptr, nullptr};
+  double2* B[2] = {nullptr, nullptr};
+  bool have_A[2] = {false, false}, have_Ainv[2] = {false, false}, have_B[2] = {false, false};
+  CloverPtr aee_s[3], ainv_oo_s[3];
+  bool clover_s_ok[3] = {false, false, false};
+
+  std::vector<double2*> s64;
+  std::vector<SpinorPtr> s32, s16;
+
+  RedScratch red{};
+  double* dres = nullptr;        // device result scalars [16]
+  double* hres = nullptr;        // pinned mirror
+  CgScalars* dcg = nullptr;
+  CgScalars* hcg = nullptr;      // pinned
+
+  double* pgen = nullptr;        // device momenta (GENERATOR_FIELD layout)
+  double2* wbuf = nullptr;       // 6 planes x 9 complex per site
+  double2* tmpclov = nullptr;    // one parity of clover blocks
+
+  std::map<int, double2*> fields;
+  int next_handle = 1;
+
+  unsigned long long seed = 48131768981101ull;  // ranf.F90:36 default seed
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> kev;  // kernel-timing event pairs
+
+  size_t spin_bytes(Prec p) const {
+    size_t st = (size_t)g.stride;
+    if (p == Prec::F64) return 12 * 16 * st;
+    if (p == Prec::F32) return 6 * 16 * st;
+    return 3 * 16 * st;
+  }
+
+  cudaError_t alloc(void** p, size_t n) {
+    cudaError_t e = cudaMalloc(p, n);
+    if (e == cudaSuccess) {
+      allocations.push_back(*p);
+      bytes += (long long)n;
+    }
+    return e;
+  }
+  double2* sp64(size_t k) {
+    while (s64.size() <= k) {
+      void* p = nullptr;
+      if (alloc(&p, spin_bytes(Prec::F64)) != cudaSuccess) return nullptr;
+      cudaMemsetAsync(p, 0, spin_bytes(Prec::F64), stream);
+      s64.push_back((double2*)p);
+    }
+    return s64[k];
+  }
+  SpinorPtr sp(Prec p, size_t k) {
+    if (p == Prec::F64) {
+      SpinorPtr r;
+      r.v = sp64(k);
+      return r;
+    }
+    auto& pool = p == Prec::F32 ? s32 : s16;
+    while (pool.size() <= k) {
+      SpinorPtr r;
+      if (alloc(&r.v, spin_bytes(p)) != cudaSuccess) return SpinorPtr{};
+      cudaMemsetAsync(r.v, 0, spin_bytes(p), stream);
+      if (p == Prec::F16) {
+        if (alloc((void**)&r.norm, sizeof(float) * g.stride) != cudaSuccess) return SpinorPtr{};
+        cudaMemsetAsync(r.norm, 0, sizeof(float) * g.stride, stream);
+      }
+      pool.push_back(r);
+    }
+    return pool[k];
+  }
+};
+
+namespace {
+
+SpinorPtr S(double2* p) {
+  SpinorPtr r;
+  r.v = p;
+  return r;
+}
+CloverPtr C(double2* p) {
+  CloverPtr r;
+  r.v = p;
+  return r;
+}
+
+#define CK(x)                                      \
+  do {                                             \
+    cudaError_t e_ = (x);                          \
+    if (e_ != cudaSuccess) return status_from_cuda(e_); \
+  } while (0)
+#define CKL() CK(cudaGetLastError())
+
+int upload_spinor(bqcdg_ctx* c, const double* host, double2* dev) {
+  size_t n = (size_t)c->g.volh * 12 * sizeof(double2);
+  CK(cudaMemcpyAsync(c->staging, host, n, cudaMemcpyHostToDevice, c->stream));
+  launch_spinor_from_fortran(c->g, dev, c->staging, c->stream);
+  CKL();
+  return BQCDG_OK;
+}
+
+int download_spinor(bqcdg_ctx* c, const double2* dev, double* host) {
+  size_t n = (size_t)c->g.volh * 12 * sizeof(double2);
+  launch_spinor_to_fortran(c->g, c->staging, dev, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(host, c->staging, n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+OpParams op_of(const bqcdg_params* p, bool with_rho) {
+  OpParams o;
+  o.kappa = p->kappa;
+  o.csw_kappa = p->csw_kappa;
+  o.h = p->h;
+  o.rho = with_rho ? p->rho : 0.0;
+  return o;
+}
+
+// sloppy copies of the links / clover blocks used by M~
+int ensure_sloppy(bqcdg_ctx* c, Prec p, bool need_clover) {
+  int k = (int)p;
+  if (!c->gauge_s_ok[k]) {
+    if (!c->gauge_su3) return BQCDG_ENOTSU3;
+    if (!c->gauge_s[k]) {
+      size_t n = (size_t)8 * 3 * c->g.stride * (p == Prec::F32 ? 16 : 8);
+      CK(c->alloc(&c->gauge_s[k], n));
+    }
+    launch_gauge_demote(c->g, p, c->gauge_s[k], c->gauge64, c->stream);
+    CKL();
+    c->gauge_s_ok[k] = true;
+  }
+  if (need_clover && !c->clover_s_ok[k]) {
+    if (!c->have_A[0] || !c->have_Ainv[1]) return BQCDG_ENOCLOVER;
+    for (int w = 0; w < 2; w++) {
+      CloverPtr& cp = w == 0 ? c->aee_s[k] : c->ainv_oo_s[k];
+      if (!cp.v) {
+        size_t n = (size_t)c->g.stride * (p == Prec::F32 ? 18 * 16 : 9 * 16);
+        CK(c->alloc(&cp.v, n));
+        if (p == Prec::F16) CK(c->alloc((void**)&cp.norm, sizeof(float) * c->g.stride));
+      }
+      launch_clover_demote(c->g, p, cp, w == 0 ? c->A[0] : c->Ainv[1], c->stream);
+      CKL();
+    }
+    c->clover_s_ok[k] = true;
+  }
+  return BQCDG_OK;
+}
+
+const void* gauge_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? (const void*)c->gauge64 : c->gauge_s[(int)p]; }
+CloverPtr aee_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? C(c->A[0]) : c->aee_s[(int)p]; }
+CloverPtr ainv_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? C(c->Ainv[1]) : c->ainv_oo_s[(int)p]; }
+
+int check_op(bqcdg_ctx* c, const bqcdg_params* p) {
+  if (!c || !p) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  if (p->csw_kappa != 0.0 && (!c->have_A[0] || !c->have_Ainv[1])) return BQCDG_ENOCLOVER;
+  return BQCDG_OK;
+}
+
+// out_e = M~ in_e  (dag: M~^+), with rho for W; t_o scratch (odd)
+void apply_mtil(bqcdg_ctx* c, Prec p, bool dag, SpinorPtr out, SpinorPtr in, SpinorPtr t, const OpParams& op,
+                double* norm_out, CgScalars* cg) {
+  launch_mtil_pass1(p, c->g, dag, t, in, gauge_of(c, p), ainv_of(c, p), op, cg, c->stream);
+  launch_mtil_pass2(p, c->g, dag, out, t, in, gauge_of(c, p), aee_of(c, p), op, c->red, norm_out, cg, c->stream);
+}
+
+// out = (W^+ W) in in precision p; scratch t (odd), q (even)
+void apply_mdagm(bqcdg_ctx* c, Prec p, SpinorPtr out, SpinorPtr in, SpinorPtr t, SpinorPtr q, const OpParams& op) {
+  apply_mtil(c, p, false, q, in, t, op, nullptr, nullptr);
+  apply_mtil(c, p, true, out, q, t, op, nullptr, nullptr);
+}
+
+int read_cg(bqcdg_ctx* c) {
+  CK(cudaMemcpyAsync(c->hcg, c->dcg, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+int write_cg(bqcdg_ctx* c) {
+  CK(cudaMemcpyAsync(c->dcg, c->hcg, sizeof(CgScalars), cudaMemcpyHostToDevice, c->stream));
+  return BQCDG_OK;
+}
+
+struct KernelTimer {
+  bqcdg_ctx* c;
+  bool on;
+  std::vector<cudaEvent_t> pending;
+  double ms = 0.0;
+  int launches = 0;
+  void begin() {
+    if (!on) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, c->stream);
+    pending.push_back(e);
+  }
+  void end() { begin(); }
+  void collect() {
+    if (!on) return;
+    cudaStreamSynchronize(c->stream);
+    for (size_t k = 0; k + 1 < pending.size(); k += 2) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, pending[k], pending[k + 1]);
+      ms += t;
+      launches++;
+    }
+    for (auto e : pending) cudaEventDestroy(e);
+    pending.clear();
+  }
+};
+
+// Core CG on device-resident x, b (F64, device layout).  Solves (W^+W) x = b.
+//   sloppy == F64: plain FP64 CG (cg.F90)
+//   otherwise:     sloppy iterations in precision `sloppy` with FP64 reliable
+//                  updates (x += x_s; r = b - A x in FP64) whenever |r| has
+//                  dropped by `delta` since the previous one, and at the end.
+int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec sloppy, int maxiter, double stop_rtr,
+            double delta, bool min_one_iter, bool time_kernels, bqcdg_solve_info* info) {
+  const Geom& g = c->g;
+  const bool clover = op.csw_kappa != 0.0;
+  if (sloppy != Prec::F64) {
+    int st = ensure_sloppy(c, sloppy, clover);
+    if (st) return st;
+  }
+  double2* r = c->sp64(0);
+  double2* ax = c->sp64(1);
+  double2* t64 = c->sp64(2);
+  double2* q64 = c->sp64(3);
+  if (!r || !ax || !t64 || !q64) return BQCDG_ENOMEM;
+  SpinorPtr p, t, q, rs, xs;
+  if (sloppy == Prec::F64) {
+    p = S(c->sp64(4));
+    t = S(t64);
+    q = S(q64);
+    rs = S(r);
+    xs = S(x);
+    if (!p.v) return BQCDG_ENOMEM;
+  } else {
+    p = c->sp(sloppy, 0);
+    t = c->sp(sloppy, 1);
+    q = c->sp(sloppy, 2);
+    rs = c->sp(Prec::F32, sloppy == Prec::F32 ? 3 : 0);
+    xs = c->sp(Prec::F32, sloppy == Prec::F32 ? 4 : 1);
+    if (!p.v || !t.v || !q.v || !rs.v || !xs.v) return BQCDG_ENOMEM;
+  }
+  KernelTimer kt{c, time_kernels};
+  CK(cudaEventRecord(c->ev0, c->stream));
+
+  // r = b - A x
+  apply_mdagm(c, Prec::F64, S(ax), S(x), S(t64), S(q64), op);
+  if (sloppy == Prec::F64) launch_residual(g, r, b, ax, Prec::F64, p, c->red, c->dres, c->stream);
+  else launch_residual(g, r, b, ax, Prec::F32, rs, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double rtr = c->hres[0];
+  info->b2 = c->hres[1];
+  if (sloppy != Prec::F64) {
+    launch_spinor_convert(g, sloppy, p, Prec::F32, rs, c->stream);
+    launch_zero(g, Prec::F32, xs, c->stream);
+    CKL();
+  }
+  CgScalars& h = *c->hcg;
+  std::memset(&h, 0, sizeof(h));
+  h.rtr = rtr;
+  h.rtr_old = rtr;
+  h.stop_rtr = stop_rtr;
+  h.maxiter = maxiter;
+  h.ru_rtr = sloppy == Prec::F64 ? -1.0 : delta * delta * rtr;
+  double maxr2 = rtr;
+  int ru = 0;
+  int nl = 5 + (sloppy != Prec::F64 ? 2 : 0);  // kernels launched so far
+  bool converged = false;
+  if (!(rtr == rtr)) h.done = 4;
+  else if (rtr == 0.0 || (!min_one_iter && rtr <= stop_rtr)) { h.done = 1; converged = true; }
+  if (maxiter <= 0 && !h.done) h.done = 3;
+  { int st_ = write_cg(c); if (st_) return st_; }
+
+  int batch = 4;
+  while (!h.done) {
+    nl += 5 * batch;
+    for (int k = 0; k < batch; k++) {
+      // pass 1 (timed), pass 2 (+|M~p|^2 -> alpha), pass 3, pass 4 (+x,r update, |r|^2), p update
+      kt.begin();
+      launch_mtil_pass1(sloppy, g, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
+      kt.end();
+      launch_mtil_pass2(sloppy, g, false, q, t, p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
+                        c->dcg, c->stream);
+      kt.begin();
+      launch_mtil_pass1(sloppy, g, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
+      kt.end();
+      launch_cg_pass4(sloppy, g, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
+                      c->stream);
+      launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream);
+    }
+    CKL();
+    int st = read_cg(c);
+    if (st) return st;
+    kt.collect();
+    if (batch < 16) batch *= 2;
+    if (h.done == 4) break;
+    if (h.done == 0) continue;
+    if (sloppy == Prec::F64) {
+      converged = h.done == 1;
+      break;
+    }
+    // reliable update: x += x_s, r = b - A x in FP64
+    nl += 7;
+    launch_accum_x(g, x, (float4*)xs.v, c->stream);
+    apply_mdagm(c, Prec::F64, S(ax), S(x), S(t64), S(q64), op);
+    launch_residual(g, r, b, ax, Prec::F32, rs, c->red, c->dres, c->stream);
+    CKL();
+    CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    ru++;
+    double rtrue = c->hres[0];
+    if (!(rtrue == rtrue)) { h.done = 4; break; }
+    if (rtrue <= stop_rtr) { h.rtr = rtrue; converged = true; h.done = 1; break; }
+    if (h.done == 3) { h.rtr = rtrue; break; }
+    // continue from the true residual: p = r + beta p with beta = |r|^2 / |r_old|^2
+    maxr2 = rtrue;
+    h.beta = rtrue / h.rtr_old;
+    h.rtr = rtrue;
+    h.ru_rtr = delta * delta * maxr2;
+    h.done = 0;
+    { int st_ = write_cg(c); if (st_) return st_; }
+    launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream);
+    CKL();
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  info->seconds = ms * 1e-3;
+  info->niter = h.iter;
+  info->reliable_updates = ru;
+  info->kernel_launches = nl;
+  info->rtr = h.rtr;
+  info->converged = converged ? 1 : 0;
+  info->stencil_ms = kt.ms;
+  info->stencil_launches = kt.launches;
+  if (h.done == 4) return BQCDG_ENAN;
+  return BQCDG_OK;
+}
+
+int true_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, double* rtr) {
+  double2* r = c->sp64(0);
+  double2* ax = c->sp64(1);
+  apply_mdagm(c, Prec::F64, S(ax), S(x), S(c->sp64(2)), S(c->sp64(3)), op);
+  launch_residual(c->g, r, b, ax, Prec::F64, SpinorPtr{}, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *rtr = c->hres[0];
+  return BQCDG_OK;
+}
+
+Prec prec_of(int p) { return p == BQCDG_PREC_DOUBLE ? Prec::F64 : (p == BQCDG_PREC_SINGLE ? Prec::F32 : Prec::F16); }
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* bqcdg_error_string(int s) {
+  switch (s) {
+    case BQCDG_OK: return "ok";
+    case BQCDG_EINVAL: return "invalid argument";
+    case BQCDG_ECUDA: return "CUDA error";
+    case BQCDG_ENOCONV: return "no convergence";
+    case BQCDG_ENAN: return "residual is NaN";
+    case BQCDG_ENOGAUGE: return "no gauge field loaded";
+    case BQCDG_ENOCLOVER: return "clover term not loaded";
+    case BQCDG_ENOMEM: return "device out of memory";
+    case BQCDG_EUNSUPPORTED: return "unsupported parameters";
+    case BQCDG_ENOTSU3: return "links are not SU(3)";
+    case BQCDG_ENODEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+int bqcdg_create(bqcdg_ctx** out, const int L[4], const int bc[4], int device) {
+  if (!out || !L || !bc) return BQCDG_EINVAL;
+  *out = nullptr;
+  for (int d = 0; d < 4; d++)
+    if (L[d] <= 0 || L[d] % 2 || (bc[d] != 1 && bc[d] != -1)) return BQCDG_EINVAL;  // init_common.F90:67-72
+  long long vol = (long long)L[0] * L[1] * L[2] * L[3];
+  if (vol / 2 > (1LL << 30)) return BQCDG_EINVAL;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return BQCDG_ENODEVICE;
+  if (device < 0 || device >= ndev) return BQCDG_EINVAL;
+  CK(cudaSetDevice(device));
+  bqcdg_ctx* c = new bqcdg_ctx();
+  c->device = device;
+  for (int d = 0; d < 4; d++) {
+    c->g.L[d] = L[d];
+    c->g.bcsign[d] = bc[d];
+  }
+  c->g.Lxh = L[0] / 2;
+  c->g.volh = (int)(vol / 2);
+  c->g.stride = (c->g.volh + 63) / 64 * 64;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  c->staging_bytes = (size_t)c->g.volh * 72 * sizeof(double2);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->staging, c->staging_bytes);
+  c->red.maxblocks = nblocks(c->g.volh);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->red.partial, sizeof(double) * 4 * c->red.maxblocks);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->red.counter, sizeof(unsigned int) * 4);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->red.counter, 0, sizeof(unsigned int) * 4, c->stream);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->dres, sizeof(double) * 16);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->dcg, sizeof(CgScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hres, sizeof(double) * 16);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hcg, sizeof(CgScalars));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    bqcdg_destroy(c);
+    return status_from_cuda(e);
+  }
+  *out = c;
+  return BQCDG_OK;
+}
+
+int bqcdg_destroy(bqcdg_ctx* c) {
+  if (!c) return BQCDG_EINVAL;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : c->allocations) cudaFree(p);
+  if (c->hres) cudaFreeHost(c->hres);
+  if (c->hcg) cudaFreeHost(c->hcg);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return BQCDG_OK;
+}
+
+int bqcdg_volh(const bqcdg_ctx* c) { return c ? c->g.volh : -1; }
+long long bqcdg_device_bytes(const bqcdg_ctx* c) { return c ? c->bytes : -1; }
+
+int bqcdg_load_gauge(bqcdg_ctx* c, const double* u, int flipped) {
+  if (!c || !u) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
+  size_t n = (size_t)c->g.volh * 72 * sizeof(double2);
+  CK(cudaMemcpyAsync(c->staging, u, n, cudaMemcpyHostToDevice, c->stream));
+  launch_gauge_from_fortran(c->g, c->gauge64, c->staging, flipped, c->stream);
+  CKL();
+  launch_gauge_check(c->g, c->gauge64, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->gauge_su3 = c->hres[0] < 1e-10 && c->hres[1] < 1e-10;
+  c->have_gauge = true;
+  for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  return BQCDG_OK;
+}
+
+int bqcdg_get_gauge(bqcdg_ctx* c, double* u, int flipped) {
+  if (!c || !u) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  launch_gauge_to_fortran(c->g, c->staging, c->gauge64, flipped, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(u, c->staging, (size_t)c->g.volh * 72 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+static int load_clover_field(bqcdg_ctx* c, double2** dst, bool* have, const double* src) {
+  for (int eo = 0; eo < 2; eo++) {
+    if (!dst[eo]) CK(c->alloc((void**)&dst[eo], (size_t)36 * c->g.stride * sizeof(double2)));
+    size_t n = (size_t)c->g.volh * 36 * sizeof(double2);
+    CK(cudaMemcpyAsync(c->staging, src + (size_t)eo * c->g.volh * 72, n, cudaMemcpyHostToDevice, c->stream));
+    launch_clover_from_fortran(c->g, dst[eo], c->staging, c->stream);
+    CKL();
+    have[eo] = true;
+  }
+  return BQCDG_OK;
+}
+
+int bqcdg_load_clover(bqcdg_ctx* c, const double* a, const double* ainv, const double* b) {
+  if (!c) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  int st;
+  if (a && (st = load_clover_field(c, c->A, c->have_A, a))) return st;
+  if (ainv && (st = load_clover_field(c, c->Ainv, c->have_Ainv, ainv))) return st;
+  if (b && (st = load_clover_field(c, c->B, c->have_B, b))) return st;
+  // an inverse is needed by M~; derive it from B when only B was given
+  if (!ainv && b) {
+    for (int eo = 0; eo < 2; eo++) {
+      if (!c->Ainv[eo]) CK(c->alloc((void**)&c->Ainv[eo], (size_t)36 * c->g.stride * sizeof(double2)));
+      launch_ainv_from_b(c->g, c->Ainv[eo], c->B[eo], c->stream);
+      CKL();
+      c->have_Ainv[eo] = true;
+    }
+  }
+  for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+static int get_clover_field(bqcdg_ctx* c, double2** srcs, const bool* have, double* dst) {
+  for (int eo = 0; eo < 2; eo++) {
+    if (!have[eo]) return BQCDG_ENOCLOVER;
+    launch_clover_to_fortran(c->g, c->staging, srcs[eo], c->stream);
+    CKL();
+    CK(cudaMemcpyAsync(dst + (size_t)eo * c->g.volh * 72, c->staging, (size_t)c->g.volh * 36 * sizeof(double2),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return BQCDG_OK;
+}
+
+int bqcdg_get_clover(bqcdg_ctx* c, double* a, double* ainv, double* b) {
+  if (!c) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  int st;
+  if (a && (st = get_clover_field(c, c->A, c->have_A, a))) return st;
+  if (ainv && (st = get_clover_field(c, c->Ainv, c->have_Ainv, ainv))) return st;
+  if (b && (st = get_clover_field(c, c->B, c->have_B, b))) return st;
+  return BQCDG_OK;
+}
+
+int bqcdg_clover_init(bqcdg_ctx* c, double csw_kappa) {
+  if (!c) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  size_t n = (size_t)36 * c->g.stride * sizeof(double2);
+  for (int eo = 0; eo < 2; eo++) {
+    if (!c->A[eo]) CK(c->alloc((void**)&c->A[eo], n));
+    if (!c->Ainv[eo]) CK(c->alloc((void**)&c->Ainv[eo], n));
+    if (!c->B[eo]) CK(c->alloc((void**)&c->B[eo], n));
+  }
+  launch_clover_init(c->g, c->gauge64, csw_kappa, c->A, c->Ainv, c->B, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  for (int eo = 0; eo < 2; eo++) c->have_A[eo] = c->have_Ainv[eo] = c->have_B[eo] = true;
+  for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  return BQCDG_OK;
+}
+
+int bqcdg_clover_action(bqcdg_ctx* c, int eo, double* action) {
+  if (!c || !action || eo < 0 || eo > 1) return BQCDG_EINVAL;
+  if (!c->have_B[eo]) return BQCDG_ENOCLOVER;
+  CK(cudaSetDevice(c->device));
+  launch_clover_action(c->g, c->B[eo], c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *action = c->hres[0];
+  return BQCDG_OK;
+}
+
+static int dslash_host(bqcdg_ctx* c, int e, int o, double* out, const double* in, bool dag) {
+  if (!c || !out || !in || e < 0 || e > 1 || o != 1 - e) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  double2* si = c->sp64(0);
+  double2* so = c->sp64(1);
+  if (!si || !so) return BQCDG_ENOMEM;
+  int st = upload_spinor(c, in, si);
+  if (st) return st;
+  launch_dslash(Prec::F64, c->g, e, dag, S(so), S(si), c->gauge64, c->stream);
+  CKL();
+  return download_spinor(c, so, out);
+}
+
+int bqcdg_d(bqcdg_ctx* c, int e, int o, double* out, const double* in) { return dslash_host(c, e, o, out, in, false); }
+int bqcdg_d_dag(bqcdg_ctx* c, int e, int o, double* out, const double* in) {
+  return dslash_host(c, e, o, out, in, true);
+}
+
+static int clover_host(bqcdg_ctx* c, int eo, double* out, const double* in, int which) {
+  if (!c || !out || !in || eo < 0 || eo > 1) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  double2* si = c->sp64(0);
+  if (!si) return BQCDG_ENOMEM;
+  double2* blk = which == 0 ? c->A[eo] : (which == 1 ? c->Ainv[eo] : c->B[eo]);
+  bool have = which == 0 ? c->have_A[eo] : (which == 1 ? c->have_Ainv[eo] : c->have_B[eo]);
+  if (!have) return BQCDG_ENOCLOVER;
+  int st = upload_spinor(c, in, si);
+  if (st) return st;
+  if (which == 2) launch_clover_mult_b(c->g, si, blk, c->stream);
+  else launch_clover_mult(Prec::F64, c->g, S(si), S(si), C(blk), c->stream);
+  CKL();
+  return download_spinor(c, si, out);
+}
+
+int bqcdg_clover_mult_a(bqcdg_ctx* c, int eo, double* out, const double* in) { return clover_host(c, eo, out, in, 0); }
+int bqcdg_clover_mult_ao(bqcdg_ctx* c, int eo, double* x) { return clover_host(c, eo, x, x, 1); }
+int bqcdg_clover_mult_b(bqcdg_ctx* c, int eo, double* x) { return clover_host(c, eo, x, x, 2); }
+
+// which: 0 mtil, 1 mtil_dag, 2 mtdagmt, 3 w_mult, 4 w_mult_dag, 5 w_dagger_w
+static int op_host(bqcdg_ctx* c, double* out, const double* in, const bqcdg_params* p, int which) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!out || !in) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  double2 *si = c->sp64(0), *so = c->sp64(1), *t = c->sp64(2), *q = c->sp64(3);
+  if (!si || !so || !t || !q) return BQCDG_ENOMEM;
+  if ((st = upload_spinor(c, in, si))) return st;
+  OpParams op = op_of(p, which >= 3);
+  switch (which) {
+    case 0: case 3: apply_mtil(c, Prec::F64, false, S(so), S(si), S(t), op, nullptr, nullptr); break;
+    case 1: case 4: apply_mtil(c, Prec::F64, true, S(so), S(si), S(t), op, nullptr, nullptr); break;
+    default: apply_mdagm(c, Prec::F64, S(so), S(si), S(t), S(q), op);
+  }
+  CKL();
+  return download_spinor(c, so, out);
+}
+
+int bqcdg_mtil(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) { return op_host(c, o, i, p, 0); }
+int bqcdg_mtil_dag(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) { return op_host(c, o, i, p, 1); }
+int bqcdg_mtdagmt(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) { return op_host(c, o, i, p, 2); }
+int bqcdg_w_mult(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) { return op_host(c, o, i, p, 3); }
+int bqcdg_w_mult_dag(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) {
+  return op_host(c, o, i, p, 4);
+}
+int bqcdg_w_dagger_w(bqcdg_ctx* c, double* o, const double* i, const bqcdg_params* p) {
+  return op_host(c, o, i, p, 5);
+}
+
+void bqcdg_solver_opts_default(bqcdg_solver_opts* o) {
+  if (!o) return;
+  o->precision = BQCDG_PREC_HALF;
+  o->maxiter = 100000;
+  o->relative = 1;
+  o->tol = 1e-10;
+  o->delta = 0.1;
+  o->check_true_residual = 1;
+  o->time_kernels = 0;
+}
+
+// x, b device-resident; solver core + optional true-residual check
+static int solve_resident(bqcdg_ctx* c, double2* x, double2* b, const bqcdg_params* p, const bqcdg_solver_opts* o,
+                          bqcdg_solve_info* info) {
+  bqcdg_solve_info tmp;
+  if (!info) info = &tmp;
+  std::memset(info, 0, sizeof(*info));
+  OpParams op = op_of(p, true);
+  Prec sl = prec_of(o->precision);
+  double stop;
+  if (o->relative) {
+    // needs |b|^2 first: computed by the residual kernel inside cg_core; use a
+    // pre-pass so the stop is known before the first iteration
+    launch_norm2(c->g, b, c->red, c->dres, c->stream);
+    CKL();
+    CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    stop = o->tol * o->tol * c->hres[0];
+  } else {
+    stop = o->tol;
+  }
+  int st = cg_core(c, x, b, op, sl, o->maxiter, stop, o->delta, false, o->time_kernels != 0, info);
+  if (st) return st;
+  info->kernel_launches += o->relative ? 1 : 0;
+  if (o->check_true_residual) {
+    info->kernel_launches += 5;
+    st = true_residual(c, x, b, op, &info->true_rtr);
+    if (st) return st;
+    info->converged = info->true_rtr <= stop ? 1 : 0;
+  }
+  return info->converged ? BQCDG_OK : BQCDG_ENOCONV;
+}
+
+int bqcdg_solve(bqcdg_ctx* c, double* x, const double* b, const bqcdg_params* p, const bqcdg_solver_opts* o,
+                bqcdg_solve_info* info) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!x || !b || !o) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  double2* dx = c->sp64(5);
+  double2* db = c->sp64(6);
+  if (!dx || !db) return BQCDG_ENOMEM;
+  if ((st = upload_spinor(c, x, dx))) return st;
+  if ((st = upload_spinor(c, b, db))) return st;
+  int rs = solve_resident(c, dx, db, p, o, info);
+  if (rs != BQCDG_OK && rs != BQCDG_ENOCONV) return rs;
+  if ((st = download_spinor(c, dx, x))) return st;
+  return rs;
+}
+
+int bqcdg_cg(bqcdg_ctx* c, double* x, const double* b, const bqcdg_params* p, const bqcdg_cg_para* cgp,
+             int* iterations, bqcdg_solve_info* info) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!x || !b || !cgp) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  bqcdg_solve_info tmp;
+  if (!info) info = &tmp;
+  std::memset(info, 0, sizeof(*info));
+  double2* dx = c->sp64(5);
+  double2* db = c->sp64(6);
+  if (!dx || !db) return BQCDG_ENOMEM;
+  if ((st = upload_spinor(c, x, dx))) return st;
+  if ((st = upload_spinor(c, b, db))) return st;
+  OpParams op = op_of(p, true);
+  st = cg_core(c, dx, db, op, Prec::F64, cgp->maxiter, (double)cgp->rest, 0.0, true, false, info);
+  if (st) return st;
+  if (iterations) *iterations = info->niter;
+  if ((st = download_spinor(c, dx, x))) return st;
+  if (!info->converged && cgp->log != 2) return BQCDG_ENOCONV;
+  return BQCDG_OK;
+}
+
+int bqcdg_quda_solver(bqcdg_ctx* c, double* x, const double* b, const bqcdg_params* p, const bqcdg_cg_para* cgp,
+                      int* iterations, bqcdg_solve_info* info) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!x || !b || !cgp) return BQCDG_EINVAL;
+  if (p->h != 0.0) return BQCDG_EUNSUPPORTED;  // invert_quda.F90:298-301
+  CK(cudaSetDevice(c->device));
+  bqcdg_solve_info tmp;
+  if (!info) info = &tmp;
+  std::memset(info, 0, sizeof(*info));
+  double2* dx = c->sp64(5);
+  double2* db = c->sp64(6);
+  if (!dx || !db) return BQCDG_ENOMEM;
+  if ((st = upload_spinor(c, x, dx))) return st;
+  if ((st = upload_spinor(c, b, db))) return st;
+  OpParams op = op_of(p, true);
+  // QUDA stops on |r| < sqrt(rest) (L2 absolute, invert_quda.F90:143,342)
+  Prec sl = c->gauge_su3 ? Prec::F16 : Prec::F64;
+  st = cg_core(c, dx, db, op, sl, cgp->maxiter, (double)cgp->rest, 0.1, false, false, info);
+  if (st) return st;
+  // host-side check of invert_quda.F90:155-168, done in FP64 on the device
+  if ((st = true_residual(c, dx, db, op, &info->true_rtr))) return st;
+  info->converged = info->true_rtr <= (double)cgp->rest ? 1 : 0;
+  if (iterations) *iterations = info->niter;
+  if ((st = download_spinor(c, dx, x))) return st;
+  if (!info->converged && cgp->log != 2) return BQCDG_ENOCONV;
+  return BQCDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// forces
+// ---------------------------------------------------------------------------
+static int ensure_force_bufs(bqcdg_ctx* c) {
+  if (!c->pgen) CK(c->alloc((void**)&c->pgen, (size_t)64 * c->g.volh * sizeof(double)));
+  if (!c->wbuf) CK(c->alloc((void**)&c->wbuf, (size_t)54 * c->g.stride * sizeof(double2)));
+  return BQCDG_OK;
+}
+
+static int apply_odd_clover_inverse(bqcdg_ctx* c, double2* x) {
+  // clover_mult_b(conf%b(ODD), x) (dsf.F90:69-70); the explicit inverse when
+  // only conf%i is resident
+  if (c->have_B[1]) launch_clover_mult_b(c->g, x, c->B[1], c->stream);
+  else if (c->have_Ainv[1]) launch_clover_mult(Prec::F64, c->g, S(x), S(x), C(c->Ainv[1]), c->stream);
+  else return BQCDG_ENOCLOVER;
+  CKL();
+  return BQCDG_OK;
+}
+
+int bqcdg_dsf(bqcdg_ctx* c, double* p, double step, const bqcdg_params* par, const double* a, const double* b) {
+  if (!c || !p || !par || !a || !b) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  int st = ensure_force_bufs(c);
+  if (st) return st;
+  double2 *da = c->sp64(0), *db = c->sp64(1), *dat = c->sp64(2), *dbt = c->sp64(3);
+  if (!da || !db || !dat || !dbt) return BQCDG_ENOMEM;
+  size_t pn = (size_t)64 * c->g.volh * sizeof(double);
+  CK(cudaMemcpyAsync(c->pgen, p, pn, cudaMemcpyHostToDevice, c->stream));
+  if ((st = upload_spinor(c, a, da))) return st;
+  if ((st = upload_spinor(c, b, db))) return st;
+  if (par->kappa != 0.0) {
+    launch_dslash(Prec::F64, c->g, 1, false, S(dat), S(da), c->gauge64, c->stream);  // A~ = D_oe A
+    launch_dslash(Prec::F64, c->g, 1, true, S(dbt), S(db), c->gauge64, c->stream);   // B~ = D_eo^+ B
+    CKL();
+    if (par->csw_kappa != 0.0) {
+      if ((st = apply_odd_clover_inverse(c, dat))) return st;
+      if ((st = apply_odd_clover_inverse(c, dbt))) return st;
+    }
+    if (par->h != 0.0) {
+      launch_h_mult_b(c->g, dat, -par->h, c->stream);
+      launch_h_mult_b(c->g, dbt, par->h, c->stream);
+      CKL();
+    }
+  }
+  double s = -step * 2.0 * par->kappa * par->kappa / (1.0 + par->h * par->h);
+  if (s != 0.0) {
+    launch_dsf_hop(c->g, c->pgen, c->gauge64, da, db, dat, dbt, s, c->stream);
+    CKL();
+  }
+  double s1 = -step * 2.0 * (par->csw_kappa / 8.0);
+  double s2 = -step * 2.0 * (par->csw_kappa / 8.0) * par->kappa * par->kappa;
+  if (s1 != 0.0) {
+    launch_clover_bsa(c->g, c->wbuf, db, da, c->stream);
+    launch_clover_d(c->g, c->pgen, c->gauge64, c->wbuf, 0, s1, c->stream);
+    CKL();
+  }
+  if (s2 != 0.0) {
+    launch_clover_bsa(c->g, c->wbuf, dbt, dat, c->stream);
+    launch_clover_d(c->g, c->pgen, c->gauge64, c->wbuf, 1, s2, c->stream);
+    CKL();
+  }
+  CK(cudaMemcpyAsync(p, c->pgen, pn, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+int bqcdg_clover_dsf(bqcdg_ctx* c, int eo, double* p, const double* b, const double* a, double s) {
+  if (!c || !p || !b || !a || eo < 0 || eo > 1) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  int st = ensure_force_bufs(c);
+  if (st) return st;
+  double2 *da = c->sp64(0), *db = c->sp64(1);
+  if (!da || !db) return BQCDG_ENOMEM;
+  size_t pn = (size_t)64 * c->g.volh * sizeof(double);
+  CK(cudaMemcpyAsync(c->pgen, p, pn, cudaMemcpyHostToDevice, c->stream));
+  if ((st = upload_spinor(c, a, da))) return st;
+  if ((st = upload_spinor(c, b, db))) return st;
+  launch_clover_bsa(c->g, c->wbuf, db, da, c->stream);
+  launch_clover_d(c->g, c->pgen, c->gauge64, c->wbuf, eo, s, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(p, c->pgen, pn, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+int bqcdg_clover_dsd(bqcdg_ctx* c, int eo, double* p, double s) {
+  if (!c || !p || eo < 0 || eo > 1) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  if (!c->have_Ainv[eo]) return BQCDG_ENOCLOVER;
+  CK(cudaSetDevice(c->device));
+  int st = ensure_force_bufs(c);
+  if (st) return st;
+  size_t pn = (size_t)64 * c->g.volh * sizeof(double);
+  CK(cudaMemcpyAsync(c->pgen, p, pn, cudaMemcpyHostToDevice, c->stream));
+  launch_clover_ts(c->g, c->wbuf, c->Ainv[eo], c->stream);
+  launch_clover_d(c->g, c->pgen, c->gauge64, c->wbuf, eo, s, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(p, c->pgen, pn, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device-resident fields
+// ---------------------------------------------------------------------------
+int bqcdg_field_create(bqcdg_ctx* c, int* handle) {
+  if (!c || !handle) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  void* p = nullptr;
+  CK(c->alloc(&p, c->spin_bytes(Prec::F64)));
+  CK(cudaMemsetAsync(p, 0, c->spin_bytes(Prec::F64), c->stream));
+  *handle = c->next_handle++;
+  c->fields[*handle] = (double2*)p;
+  return BQCDG_OK;
+}
+
+static double2* field(bqcdg_ctx* c, int h) {
+  auto it = c->fields.find(h);
+  return it == c->fields.end() ? nullptr : it->second;
+}
+
+int bqcdg_field_upload(bqcdg_ctx* c, int h, const double* host) {
+  if (!c || !host || !field(c, h)) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  int st = upload_spinor(c, host, field(c, h));
+  if (st) return st;
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+int bqcdg_field_download(bqcdg_ctx* c, int h, double* host) {
+  if (!c || !host || !field(c, h)) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return download_spinor(c, field(c, h), host);
+}
+
+int bqcdg_field_destroy(bqcdg_ctx* c, int h) {
+  if (!c || !field(c, h)) return BQCDG_EINVAL;
+  // memory stays in the context pool until bqcdg_destroy
+  c->fields.erase(h);
+  return BQCDG_OK;
+}
+
+int bqcdg_field_gauss(bqcdg_ctx* c, int h, double var) {
+  if (!c || !field(c, h)) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  launch_ran_gauss(c->staging, c->g.volh, 12, var, c->seed, c->stream);
+  c->seed = ranf_skip(c->seed, 2ull * 12ull * (unsigned long long)c->g.volh);
+  launch_spinor_from_fortran(c->g, field(c, h), c->staging, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// seeded gauge fields
+// ---------------------------------------------------------------------------
+int bqcdg_ranset(bqcdg_ctx* c, long long seed, long long skip) {
+  if (!c) return BQCDG_EINVAL;
+  const unsigned long long M48 = 281474976710655ull;
+  c->seed = seed == 0 ? 48131768981101ull : (((unsigned long long)seed | 1ull) & M48);
+  c->seed = ranf_skip(c->seed, (unsigned long long)skip & M48);
+  return BQCDG_OK;
+}
+
+int bqcdg_ranget(bqcdg_ctx* c, long long* seed) {
+  if (!c || !seed) return BQCDG_EINVAL;
+  *seed = (long long)c->seed;
+  return BQCDG_OK;
+}
+
+static int gauge_finish(bqcdg_ctx* c) {
+  launch_gauge_from_fortran(c->g, c->gauge64, c->staging, 0, c->stream);
+  CKL();
+  launch_gauge_check(c->g, c->gauge64, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->gauge_su3 = c->hres[0] < 1e-10 && c->hres[1] < 1e-10;
+  c->have_gauge = true;
+  for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  return BQCDG_OK;
+}
+
+int bqcdg_conf_hot(bqcdg_ctx* c) {
+  if (!c) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
+  const unsigned long long per = 2ull * 9ull * (unsigned long long)c->g.volh;
+  for (int me = 0; me < 8; me++) {  // do mu; do eo (conf.F90:208-214)
+    launch_ran_gauss(c->staging + (size_t)me * c->g.volh * 9, c->g.volh, 9, 1.0, c->seed, c->stream);
+    c->seed = ranf_skip(c->seed, per);
+  }
+  launch_u_normalize(c->staging, 8LL * c->g.volh, c->stream);
+  CKL();
+  return gauge_finish(c);
+}
+
+int bqcdg_conf_cold(bqcdg_ctx* c) {
+  if (!c) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
+  launch_cold(c->staging, 8LL * c->g.volh, c->stream);
+  CKL();
+  return gauge_finish(c);
+}
+
+int bqcdg_conf_relax(bqcdg_ctx* c, int n) {
+  if (!c || n < 0) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  for (int k = 0; k < n; k++) launch_conf_relax(c->g, c->gauge64, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  return BQCDG_OK;
+}
+
+int bqcdg_sg(bqcdg_ctx* c, double* sg) {
+  if (!c || !sg) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  launch_plaquette(c->g, c->gauge64, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *sg = 6.0 * 2.0 * c->g.volh - c->hres[0] / 3.0;
+  return BQCDG_OK;
+}
+
+int bqcdg_solve_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const bqcdg_solver_opts* o,
+                    bqcdg_solve_info* info) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!o || !field(c, hx) || !field(c, hb)) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  return solve_resident(c, field(c, hx), field(c, hb), p, o, info);
+}
+
+int bqcdg_mdagm_dev(bqcdg_ctx* c, int hout, int hin, const bqcdg_params* p, int precision, int n, double* ms) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!field(c, hout) || !field(c, hin) || n <= 0) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  Prec pr = prec_of(precision);
+  OpParams op = op_of(p, true);
+  SpinorPtr in, out, t, q;
+  if (pr == Prec::F64) {
+    in = S(field(c, hin));
+    out = S(field(c, hout));
+    t = S(c->sp64(2));
+    q = S(c->sp64(3));
+  } else {
+    if ((st = ensure_sloppy(c, pr, p->csw_kappa != 0.0))) return st;
+    in = c->sp(pr, 5);
+    out = c->sp(pr, 6);
+    t = c->sp(pr, 7);
+    q = c->sp(pr, 8);
+    launch_spinor_convert(c->g, pr, in, Prec::F64, S(field(c, hin)), c->stream);
+  }
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int k = 0; k < n; k++) apply_mdagm(c, pr, out, in, t, q, op);
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CKL();
+  if (pr != Prec::F64) launch_spinor_convert(c->g, Prec::F64, S(field(c, hout)), pr, out, c->stream);
+  CK(cudaStreamSynchronize(c->stream));
+  float t_ms = 0.f;
+  cudaEventElapsedTime(&t_ms, c->ev0, c->ev1);
+  if (ms) *ms = t_ms / n;
+  return BQCDG_OK;
+}
+
+int bqcdg_time_pass(bqcdg_ctx* c, int hin, const bqcdg_params* p, int precision, int n, double* ms) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!field(c, hin) || n <= 0) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  Prec pr = prec_of(precision);
+  OpParams op = op_of(p, true);
+  SpinorPtr in, t;
+  if (pr == Prec::F64) {
+    in = S(field(c, hin));
+    t = S(c->sp64(2));
+  } else {
+    if ((st = ensure_sloppy(c, pr, p->csw_kappa != 0.0))) return st;
+    in = c->sp(pr, 5);
+    t = c->sp(pr, 7);
+    launch_spinor_convert(c->g, pr, in, Prec::F64, S(field(c, hin)), c->stream);
+  }
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int k = 0; k < n; k++)
+    launch_mtil_pass1(pr, c->g, false, t, in, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream);
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  float t_ms = 0.f;
+  cudaEventElapsedTime(&t_ms, c->ev0, c->ev1);
+  if (ms) *ms = t_ms / n;
+  return BQCDG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,222 @@
+// clover_init.cu -- clover term construction on the device (FP64):
+//   clover_f_mu_nu.F90:37-103  four-leaf field strength per plane
+//   clover_init.F90:28-190     A = 1 - (c_sw kappa / 8) sigma.F in two chiral 6x6 blocks
+//   clover_inv.F90:29-220      LDL^+ factors B, explicit inverse, and the halving
+//                              of A, A^-1 and 1/D
+// plus clover_action.F90:29-60 (2 sum log prod 1/D).
+#include "kernels.cuh"
+#include "su3.cuh"
+
+namespace bqcdg {
+
+// f(mu,nu) at site x (coordinates xs); closed loops, so periodic links
+__device__ void clover_f_mu_nu(const Geom& g, const double2* gauge, L64& f, int mu, int nu, const int xs[4]) {
+  int xp_[4], xm_[4], x_p[4], x_m[4], xmp[4], xmm[4], xpm[4];
+  shift(g, xs, mu, 1, xp_);
+  shift(g, xs, mu, -1, xm_);
+  shift(g, xs, nu, 1, x_p);
+  shift(g, xs, nu, -1, x_m);
+  shift(g, xm_, nu, 1, xmp);
+  shift(g, xm_, nu, -1, xmm);
+  shift(g, xp_, nu, -1, xpm);
+  L64 a, b, c, d, t, r;
+  lzero(f);
+  // uuuu1: u1 u2 u3^+ u4^+
+  load_link(g, gauge, mu, xs, a); load_link(g, gauge, nu, xp_, b); load_link(g, gauge, mu, x_p, c);
+  load_link(g, gauge, nu, xs, d);
+  mul2(t, a, false, b, false); mul3(r, t, false, c, true, d, true);
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  // uuuu2: u1 u2^+ u3^+ u4
+  load_link(g, gauge, nu, xs, a); load_link(g, gauge, mu, xmp, b); load_link(g, gauge, nu, xm_, c);
+  load_link(g, gauge, mu, xm_, d);
+  mul2(t, a, false, b, true); mul3(r, t, false, c, true, d, false);
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  // uuuu3: u1^+ u2^+ u3 u4
+  load_link(g, gauge, mu, xm_, a); load_link(g, gauge, nu, xmm, b); load_link(g, gauge, mu, xmm, c);
+  load_link(g, gauge, nu, x_m, d);
+  mul2(t, a, true, b, true); mul3(r, t, false, c, false, d, false);
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  // uuuu4: u1^+ u2 u3 u4^+
+  load_link(g, gauge, nu, x_m, a); load_link(g, gauge, mu, x_m, b); load_link(g, gauge, nu, xpm, c);
+  load_link(g, gauge, mu, xs, d);
+  mul2(t, a, true, b, false); mul3(r, t, false, c, false, d, true);
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  // clover_f_mu_nu.F90:92-102
+  C64 f10 = f.m[1][0], f20 = f.m[2][0], f21 = f.m[2][1];
+  f.m[0][0] = mkc(2.0 * f.m[0][0].y, 0.0);
+  f.m[1][1] = mkc(2.0 * f.m[1][1].y, 0.0);
+  f.m[2][2] = mkc(2.0 * f.m[2][2].y, 0.0);
+  f.m[0][1] = itimes(conjg(f10) - f.m[0][1]);
+  f.m[0][2] = itimes(conjg(f20) - f.m[0][2]);
+  f.m[1][2] = itimes(conjg(f21) - f.m[1][2]);
+  f.m[1][0] = conjg(f.m[0][1]);
+  f.m[2][0] = conjg(f.m[0][2]);
+  f.m[2][1] = conjg(f.m[1][2]);
+}
+
+// full 6x6 Hermitian block (upper triangle + real diagonal used)
+struct Blk {
+  C64 m[6][6];
+};
+
+// clover_init1 (clover_init.F90:99-120)
+__device__ __forceinline__ void init1(Blk& a, const L64& f) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    a.m[r][r] = mkc(f.m[r][r].x, 0.0);
+    a.m[r + 3][r + 3] = mkc(-f.m[r][r].x, 0.0);
+  }
+  a.m[0][1] = f.m[0][1]; a.m[0][2] = f.m[0][2]; a.m[1][2] = f.m[1][2];
+  a.m[3][4] = -a.m[0][1]; a.m[3][5] = -a.m[0][2]; a.m[4][5] = -a.m[1][2];
+}
+// clover_init2 (clover_init.F90:122-145)
+__device__ __forceinline__ void init2(Blk& a, const L64& f, const L64& gg) {
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) a.m[r][c + 3] = f.m[r][c] + itimes(gg.m[r][c]);
+}
+
+__device__ __forceinline__ C64 hel(const Blk& a, int r, int c) { return r <= c ? a.m[r][c] : conjg(a.m[c][r]); }
+
+__device__ __forceinline__ void store_packed(double2* dst, int stride, int i, int chi, const Blk& a, double scale) {
+  const int slot_up[6][6] = {{-1, 1, 2, 3, 4, 5},    {-1, -1, 6, 7, 8, 9},    {-1, -1, -1, 11, 12, 13},
+                             {-1, -1, -1, -1, 14, 15}, {-1, -1, -1, -1, -1, 17}, {-1, -1, -1, -1, -1, -1}};
+  double2* b = dst + chi * 18 * stride + i;
+  b[0] = make_double2(scale * a.m[0][0].x, scale * a.m[1][1].x);
+  b[10 * stride] = make_double2(scale * a.m[2][2].x, scale * a.m[3][3].x);
+  b[16 * stride] = make_double2(scale * a.m[4][4].x, scale * a.m[5][5].x);
+  for (int r = 0; r < 6; r++)
+    for (int c = r + 1; c < 6; c++)
+      b[slot_up[r][c] * stride] = make_double2(scale * a.m[r][c].x, scale * a.m[r][c].y);
+}
+
+// clover_inv (clover_inv.F90:29-220) on an unhalved block a; writes the
+// halved A, the halved inverse and the B factors (L, halved 1/D)
+__device__ void block_inv(const Blk& a, double2* A, double2* Ainv, double2* B, int stride, int i, int chi) {
+  C64 L[6][6];
+  double d[6], dinv[6];
+  for (int r = 0; r < 6; r++) {
+    C64 tmp[6];
+    for (int c = 0; c < r; c++) {
+      C64 t = hel(a, r, c);
+      for (int k = 0; k < c; k++) t = t - tmp[k] * conjg(L[c][k]);
+      tmp[c] = t;
+    }
+    for (int c = 0; c < r; c++) L[r][c] = dinv[c] * tmp[c];
+    double dr = a.m[r][r].x;
+    for (int k = 0; k < r; k++) dr = dr - d[k] * norm2(L[r][k]);
+    d[r] = dr;
+    dinv[r] = 1.0 / dr;
+  }
+  // B = (L, 1/D / 2)
+  double2* bb = B + chi * 18 * stride + i;
+  for (int r = 1; r < 6; r++)
+    for (int c = 0; c < r; c++) bb[(r * (r - 1) / 2 + c) * stride] = make_double2(L[r][c].x, L[r][c].y);
+  bb[15 * stride] = make_double2(0.5 * dinv[0], 0.5 * dinv[1]);
+  bb[16 * stride] = make_double2(0.5 * dinv[2], 0.5 * dinv[3]);
+  bb[17 * stride] = make_double2(0.5 * dinv[4], 0.5 * dinv[5]);
+  // clover_inv2: columns of A^-1 by unit solves, stored halved (upper part)
+  Blk inv;
+  for (int col = 0; col < 6; col++) {
+    C64 y[6], x[6];
+    for (int k = 0; k < 6; k++) y[k] = mkc(k == col ? 1.0 : 0.0, 0.0);
+    for (int r = 1; r < 6; r++) {
+      C64 s = y[r];
+      for (int c = 0; c < r; c++) s = s - L[r][c] * y[c];
+      y[r] = s;
+    }
+    for (int r = 5; r >= 0; r--) {
+      C64 s = dinv[r] * y[r];
+      for (int c = r + 1; c < 6; c++) s = s - conjg(L[c][r]) * x[c];
+      x[r] = s;
+    }
+    // x = column col of A^-1; row col of the Hermitian inverse is conj(x)
+    inv.m[col][col] = mkc(x[col].x, 0.0);
+    for (int k = col + 1; k < 6; k++) inv.m[col][k] = conjg(x[k]);
+  }
+  store_packed(Ainv, stride, i, chi, inv, 0.5);
+  store_packed(A, stride, i, chi, a, 0.5);
+}
+
+__global__ void __launch_bounds__(64) k_clover_init(Geom g, const double2* gauge, double factor, double2* a0,
+                                                    double2* a1, double2* ai0, double2* ai1, double2* b0,
+                                                    double2* b1) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int eo = blockIdx.y;
+  if (i >= g.volh) return;
+  Site st = site_coords(g, i, eo);
+  Blk p, q;
+  L64 f, f2;
+  // clover_init.F90:52-77 (1-based planes 21; 32,31; 34; 14,42)
+  clover_f_mu_nu(g, gauge, f, 1, 0, st.x);
+  init1(p, f);
+  clover_f_mu_nu(g, gauge, f, 2, 1, st.x);
+  clover_f_mu_nu(g, gauge, f2, 2, 0, st.x);
+  init2(p, f, f2);
+  clover_f_mu_nu(g, gauge, f, 2, 3, st.x);
+  init1(q, f);
+  clover_f_mu_nu(g, gauge, f, 0, 3, st.x);
+  clover_f_mu_nu(g, gauge, f2, 3, 1, st.x);
+  init2(q, f, f2);
+  // clover_init3: a1 = s(p+q)+1, a2 = s(p-q)+1 (upper triangle)
+  Blk bl;
+  double2* A = eo == 0 ? a0 : a1;
+  double2* AI = eo == 0 ? ai0 : ai1;
+  double2* B = eo == 0 ? b0 : b1;
+  for (int chi = 0; chi < 2; chi++) {
+    const double sg = chi == 0 ? 1.0 : -1.0;
+    for (int r = 0; r < 6; r++)
+      for (int c = r; c < 6; c++) bl.m[r][c] = factor * (p.m[r][c] + sg * q.m[r][c]);
+    for (int r = 0; r < 6; r++) bl.m[r][r] = mkc(bl.m[r][r].x + 1.0, 0.0);
+    block_inv(bl, A, AI, B, g.stride, i, chi);
+  }
+}
+
+void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, double2* a[2], double2* ainv[2],
+                        double2* b[2], cudaStream_t s) {
+  dim3 grid((g.volh + 63) / 64, 2);
+  k_clover_init<<<grid, 64, 0, s>>>(g, gauge, -csw_kappa / 8.0, a[0], a[1], ainv[0], ainv[1], b[0], b[1]);
+}
+
+__global__ void __launch_bounds__(kBlock) k_clover_action(Geom g, const double2* b, RedScratch red, double* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < g.volh) {
+    double d1 = 1.0, d2 = 1.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      double2 t1 = b[(15 + k) * g.stride + i], t2 = b[(18 + 15 + k) * g.stride + i];
+      d1 *= t1.x * t1.y;
+      d2 *= t2.x * t2.y;
+    }
+    acc[0] = log(d1 * d2);
+  }
+  block_reduce_store<1>(acc, red.partial, red.maxblocks);
+  if (last_block(red.counter)) {
+    double tot[1];
+    final_sum<1>(red.partial, red.maxblocks, tot);
+    if (threadIdx.x == 0) {
+      *out = 2.0 * tot[0];
+      *red.counter = 0;
+    }
+  }
+}
+
+void launch_clover_action(const Geom& g, const double2* b, RedScratch red, double* out, cudaStream_t s) {
+  k_clover_action<<<nblocks(g.volh), kBlock, 0, s>>>(g, b, red, out);
+}
+
+}  // namespace bqcdg

@@ -1,0 +1,443 @@
+// dslash.cu -- even/odd clover-Wilson stencil kernels for sm_100a.
+//
+// One thread per output site; every field is component-major so each load of
+// one component by a warp is one contiguous transaction.  The kernels are
+// HBM-bound (about 0.9 flop/byte in FP64), so the design goal is to touch each
+// byte once: links and clover blocks are read once per output site, the
+// neighbour spinors are re-read through L1/L2 (t-neighbours of a 32^3 slab are
+// a few MB apart, well inside the 126 MB L2), and every BLAS step of CG that
+// can be is fused into the stencil epilogue.
+#include "kernels.cuh"
+
+namespace bqcdg {
+
+template <Prec P>
+struct Views {
+  using R = typename SpinorView<P>::R;
+};
+
+template <Prec P>
+__device__ __forceinline__ SpinorView<P> sview(SpinorPtr p, int stride);
+template <>
+__device__ __forceinline__ SpinorView<Prec::F64> sview<Prec::F64>(SpinorPtr p, int stride) {
+  return SpinorView<Prec::F64>{(double2*)p.v, stride};
+}
+template <>
+__device__ __forceinline__ SpinorView<Prec::F32> sview<Prec::F32>(SpinorPtr p, int stride) {
+  return SpinorView<Prec::F32>{(float4*)p.v, stride};
+}
+template <>
+__device__ __forceinline__ SpinorView<Prec::F16> sview<Prec::F16>(SpinorPtr p, int stride) {
+  return SpinorView<Prec::F16>{(int4*)p.v, p.norm, stride};
+}
+
+template <Prec P>
+__device__ __forceinline__ GaugeView<P> gview(const void* p, int stride);
+template <>
+__device__ __forceinline__ GaugeView<Prec::F64> gview<Prec::F64>(const void* p, int stride) {
+  return GaugeView<Prec::F64>{(double2*)p, stride};
+}
+template <>
+__device__ __forceinline__ GaugeView<Prec::F32> gview<Prec::F32>(const void* p, int stride) {
+  return GaugeView<Prec::F32>{(float4*)p, stride};
+}
+template <>
+__device__ __forceinline__ GaugeView<Prec::F16> gview<Prec::F16>(const void* p, int stride) {
+  return GaugeView<Prec::F16>{(short4*)p, stride};
+}
+
+template <Prec P>
+__device__ __forceinline__ CloverView<P> cview(CloverPtr p, int stride);
+template <>
+__device__ __forceinline__ CloverView<Prec::F64> cview<Prec::F64>(CloverPtr p, int stride) {
+  return CloverView<Prec::F64>{(double2*)p.v, stride};
+}
+template <>
+__device__ __forceinline__ CloverView<Prec::F32> cview<Prec::F32>(CloverPtr p, int stride) {
+  return CloverView<Prec::F32>{(float4*)p.v, stride};
+}
+template <>
+__device__ __forceinline__ CloverView<Prec::F16> cview<Prec::F16>(CloverPtr p, int stride) {
+  return CloverView<Prec::F16>{(int4*)p.v, p.norm, stride};
+}
+
+// ---------------------------------------------------------------------------
+// plain hopping term: out(e) = D_{e,o} in(o)   (d / d_dag, d/D21.F90:29-77)
+// ---------------------------------------------------------------------------
+template <Prec P, bool DAG>
+__global__ void __launch_bounds__(kBlock) k_dslash(Geom g, int e, SpinorPtr outp, SpinorPtr inp, const void* gauge) {
+  using R = typename SpinorView<P>::R;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  auto in = sview<P>(inp, g.stride);
+  auto out = sview<P>(outp, g.stride);
+  auto U = gview<P>(gauge, g.stride);
+  Site st = site_coords(g, i, e);
+  Spinor<R> b;
+  wilson_hop<P, P, DAG>(g, e, i, st, in, U, b);
+  out.store(i, b);
+}
+
+void launch_dslash(Prec p, const Geom& g, int e, bool dag, SpinorPtr out, SpinorPtr in, const void* gauge,
+                   cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+#define DS(PP, D) k_dslash<PP, D><<<grid, kBlock, 0, s>>>(g, e, out, in, gauge)
+  if (p == Prec::F64) { if (dag) DS(Prec::F64, true); else DS(Prec::F64, false); }
+  else if (p == Prec::F32) { if (dag) DS(Prec::F32, true); else DS(Prec::F32, false); }
+  else { if (dag) DS(Prec::F16, true); else DS(Prec::F16, false); }
+#undef DS
+}
+
+// ---------------------------------------------------------------------------
+// clover multiply: out = A in  (clover_mult_a / clover_mult_ao)
+// ---------------------------------------------------------------------------
+template <Prec P>
+__global__ void __launch_bounds__(kBlock) k_clover_mult(Geom g, SpinorPtr outp, SpinorPtr inp, CloverPtr ap) {
+  using R = typename SpinorView<P>::R;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  auto in = sview<P>(inp, g.stride);
+  auto out = sview<P>(outp, g.stride);
+  auto A = cview<P>(ap, g.stride);
+  Spinor<R> x, y;
+  in.load(i, x);
+  clover_apply(A, i, x, y);
+  out.store(i, y);
+}
+
+void launch_clover_mult(Prec p, const Geom& g, SpinorPtr out, SpinorPtr in, CloverPtr a, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  if (p == Prec::F64) k_clover_mult<Prec::F64><<<grid, kBlock, 0, s>>>(g, out, in, a);
+  else if (p == Prec::F32) k_clover_mult<Prec::F32><<<grid, kBlock, 0, s>>>(g, out, in, a);
+  else k_clover_mult<Prec::F16><<<grid, kBlock, 0, s>>>(g, out, in, a);
+}
+
+// ---------------------------------------------------------------------------
+// clover_mult_b (clover_mult_b.F90 + clover_mult_b.h90): x = B^-1 x by
+// forward (L), diagonal (1/D, halved) and backward (L^+) substitution.
+// B slots: L(r,c) r>c at r(r-1)/2+c (15 complex), 1/D pairs at 15,16,17.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ldl_solve(const double2* b, int i, int stride, int chi, cx<double> y[6],
+                                          cx<double> x[6]) {
+  cx<double> L[15];
+#pragma unroll
+  for (int k = 0; k < 15; k++) {
+    double2 t = __ldg(b + (chi * 18 + k) * stride + i);
+    L[k] = mkc(t.x, t.y);
+  }
+  double dinv[6];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double2 t = __ldg(b + (chi * 18 + 15 + k) * stride + i);
+    dinv[2 * k] = t.x;
+    dinv[2 * k + 1] = t.y;
+  }
+#pragma unroll
+  for (int r = 1; r < 6; r++) {
+    cx<double> s = y[r];
+#pragma unroll
+    for (int c = 0; c < r; c++) s = s - L[r * (r - 1) / 2 + c] * y[c];
+    y[r] = s;
+  }
+#pragma unroll
+  for (int r = 5; r >= 0; r--) {
+    cx<double> s = dinv[r] * y[r];
+#pragma unroll
+    for (int c = r + 1; c < 6; c++) s = s - conjg(L[c * (c - 1) / 2 + r]) * x[c];
+    x[r] = s;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_clover_mult_b(Geom g, double2* xf, const double2* b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  SpinorView<Prec::F64> X{xf, g.stride};
+  Spinor<double> s;
+  X.load(i, s);
+  cx<double> y[6], xs[6];
+  Spinor<double> o;
+#pragma unroll
+  for (int k = 0; k < 6; k++) y[k] = s.c[k / 3][k % 3] + s.c[k / 3 + 2][k % 3];
+  ldl_solve(b, i, g.stride, 0, y, xs);
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    o.c[k / 3][k % 3] = xs[k];
+    o.c[k / 3 + 2][k % 3] = xs[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 6; k++) y[k] = s.c[k / 3][k % 3] - s.c[k / 3 + 2][k % 3];
+  ldl_solve(b, i, g.stride, 1, y, xs);
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    o.c[k / 3][k % 3] = o.c[k / 3][k % 3] + xs[k];
+    o.c[k / 3 + 2][k % 3] = o.c[k / 3 + 2][k % 3] - xs[k];
+  }
+  X.store(i, o);
+}
+
+void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStream_t s) {
+  k_clover_mult_b<<<nblocks(g.volh), kBlock, 0, s>>>(g, x, b);
+}
+
+// ---------------------------------------------------------------------------
+// mtil / mtil_dag, first half (m_tilde.F90:55-58, 92-95):
+//   t_o = Ainv_oo D_oe in_e, then (1 - i h g5) t_o for mtil, (1 + i h g5) for mtil_dag
+// ---------------------------------------------------------------------------
+template <Prec P, bool DAG>
+__global__ void __launch_bounds__(kBlock) k_pass1(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge,
+                                                  CloverPtr ainv, int has_clover, double hval, const CgScalars* cg) {
+  using R = typename SpinorView<P>::R;
+  if (cg && cg->done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  auto in = sview<P>(inp, g.stride);
+  auto out = sview<P>(outp, g.stride);
+  auto U = gview<P>(gauge, g.stride);
+  Site st = site_coords(g, i, 1);
+  Spinor<R> b;
+  wilson_hop<P, P, DAG>(g, 1, i, st, in, U, b);
+  if (has_clover) {
+    Spinor<R> y;
+    clover_apply(cview<P>(ainv, g.stride), i, b, y);
+    b = y;
+  }
+  if (hval != 0.0) h_mult_b(b, (R)hval);
+  out.store(i, b);
+}
+
+void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  int hc = op.csw_kappa != 0.0;
+  double hv = dag ? op.h : -op.h;
+#define P1(PP, D) k_pass1<PP, D><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg)
+  if (p == Prec::F64) { if (dag) P1(Prec::F64, true); else P1(Prec::F64, false); }
+  else if (p == Prec::F32) { if (dag) P1(Prec::F32, true); else P1(Prec::F32, false); }
+  else { if (dag) P1(Prec::F16, true); else P1(Prec::F16, false); }
+#undef P1
+}
+
+// core of the second half: out = A_ee x + b D_eo t (clover) or x + b D_eo t
+// (+ i h' g5 x for Wilson, h_mult.F90:27-49), + rho x  (m_tilde.F90:63-73,
+// w_mult.F90:39)
+template <Prec P, bool DAG>
+__device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorView<P>& t, const SpinorView<P>& xin,
+                                           const GaugeView<P>& U, const CloverPtr& aee, int has_clover, double bcoef,
+                                           double hval, double rho, Spinor<typename SpinorView<P>::R>& out,
+                                           Spinor<typename SpinorView<P>::R>& x) {
+  using R = typename SpinorView<P>::R;
+  Site st = site_coords(g, i, 0);
+  Spinor<R> hop;
+  wilson_hop<P, P, DAG>(g, 0, i, st, t, U, hop);
+  xin.load(i, x);
+  const R bb = (R)bcoef;
+  if (has_clover) {
+    clover_apply(cview<P>(aee, g.stride), i, x, out);
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) out.c[s][c] = out.c[s][c] + bb * hop.c[s][c];
+  } else {
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) out.c[s][c] = x.c[s][c] + bb * hop.c[s][c];
+    if (hval != 0.0) {
+      const R hh = (R)hval;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        out.c[0][c] = out.c[0][c] + hh * itimes(x.c[2][c]);
+        out.c[1][c] = out.c[1][c] + hh * itimes(x.c[3][c]);
+        out.c[2][c] = out.c[2][c] + hh * itimes(x.c[0][c]);
+        out.c[3][c] = out.c[3][c] + hh * itimes(x.c[1][c]);
+      }
+    }
+  }
+  if (rho != 0.0) {
+    const R rr = (R)rho;
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) out.c[s][c] = out.c[s][c] + rr * x.c[s][c];
+  }
+}
+
+template <Prec P, bool DAG, bool REDUCE>
+__global__ void __launch_bounds__(kBlock) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
+                                                  const void* gauge, CloverPtr aee, int has_clover, double bcoef,
+                                                  double hval, double rho, RedScratch red, double* norm_out,
+                                                  CgScalars* cg) {
+  using R = typename SpinorView<P>::R;
+  if (cg && cg->done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < g.volh) {
+    auto t = sview<P>(tp, g.stride);
+    auto xin = sview<P>(xp, g.stride);
+    auto out = sview<P>(outp, g.stride);
+    auto U = gview<P>(gauge, g.stride);
+    Spinor<R> o, x;
+    pass2_core<P, DAG>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o, x);
+    out.store(i, o);
+    if (REDUCE) {
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) acc[0] += (double)norm2(o.c[s][c]);
+    }
+  }
+  if (REDUCE) {
+    block_reduce_store<1>(acc, red.partial, red.maxblocks);
+    if (last_block(red.counter)) {
+      double tot[1];
+      final_sum<1>(red.partial, red.maxblocks, tot);
+      if (threadIdx.x == 0) {
+        if (norm_out) *norm_out = tot[0];
+        if (cg) {
+          cg->paap = tot[0];
+          cg->alpha = cg->rtr / tot[0];
+        }
+        *red.counter = 0;
+      }
+    }
+  }
+}
+
+void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
+                       const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
+                       CgScalars* cg, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  int hc = op.csw_kappa != 0.0;
+  double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
+  double hv = dag ? -op.h : op.h;
+  bool reduce = norm_out != nullptr || cg != nullptr;
+#define P2(PP, D, RR) \
+  k_pass2<PP, D, RR><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, norm_out, cg)
+#define P2R(PP, D) \
+  if (reduce) P2(PP, D, true); else P2(PP, D, false);
+  if (p == Prec::F64) { if (dag) { P2R(Prec::F64, true) } else { P2R(Prec::F64, false) } }
+  else if (p == Prec::F32) { if (dag) { P2R(Prec::F32, true) } else { P2R(Prec::F32, false) } }
+  else { if (dag) { P2R(Prec::F16, true) } else { P2R(Prec::F16, false) } }
+#undef P2R
+#undef P2
+}
+
+// ---------------------------------------------------------------------------
+// CG-fused last pass of M^+M (cg.F90:93-107 folded into mtil_dag's second half)
+// ---------------------------------------------------------------------------
+template <Prec XP>
+struct XR;
+template <>
+struct XR<Prec::F64> {
+  using View = SpinorView<Prec::F64>;
+};
+template <>
+struct XR<Prec::F32> {
+  using View = SpinorView<Prec::F32>;
+};
+
+template <Prec P, Prec XP>
+__global__ void __launch_bounds__(kBlock) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
+                                                     CloverPtr aee, int has_clover, double bcoef, double hval,
+                                                     double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
+                                                     RedScratch red, CgScalars* cg) {
+  using R = typename SpinorView<P>::R;
+  using RX = typename SpinorView<XP>::R;
+  if (cg->done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < g.volh) {
+    auto t = sview<P>(tp, g.stride);
+    auto q = sview<P>(qp, g.stride);
+    auto U = gview<P>(gauge, g.stride);
+    Spinor<R> ap, qq;
+    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap, qq);
+    auto pv = sview<P>(pp, g.stride);
+    auto xv = sview<XP>(xp, g.stride);
+    auto rv = sview<XP>(rp, g.stride);
+    Spinor<R> pl;
+    pv.load(i, pl);
+    Spinor<RX> xl, rl;
+    xv.load(i, xl);
+    rv.load(i, rl);
+    const RX a = (RX)cg->alpha;
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        cx<RX> pc = mkc((RX)pl.c[s][c].x, (RX)pl.c[s][c].y);
+        cx<RX> ac = mkc((RX)ap.c[s][c].x, (RX)ap.c[s][c].y);
+        xl.c[s][c] = xl.c[s][c] + a * pc;
+        rl.c[s][c] = rl.c[s][c] - a * ac;
+        acc[0] += (double)norm2(rl.c[s][c]);
+      }
+    xv.store(i, xl);
+    rv.store(i, rl);
+  }
+  block_reduce_store<1>(acc, red.partial, red.maxblocks);
+  if (last_block(red.counter)) {
+    double tot[1];
+    final_sum<1>(red.partial, red.maxblocks, tot);
+    if (threadIdx.x == 0) {
+      double rtr = tot[0];
+      cg->iter += 1;
+      cg->rtr_old = cg->rtr;
+      cg->rtr = rtr;
+      cg->beta = rtr / cg->rtr_old;
+      if (!(rtr == rtr)) cg->done = 4;  // NaN: stop, reported as an error
+      else if (rtr <= cg->stop_rtr) cg->done = 1;
+      else if (cg->iter >= cg->maxiter) cg->done = 3;
+      else if (rtr < cg->ru_rtr) cg->done = 2;
+      *red.counter = 0;
+    }
+  }
+}
+
+void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
+                     const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
+                     cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  int hc = op.csw_kappa != 0.0;
+  double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
+  double hv = -op.h;  // mtil_dag
+  if (p == Prec::F64)
+    k_cg_pass4<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
+                                                             x, r, red, cg);
+  else if (p == Prec::F32)
+    k_cg_pass4<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
+                                                             x, r, red, cg);
+  else
+    k_cg_pass4<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
+                                                             x, r, red, cg);
+}
+
+// p = r + beta p   (sc_xpby, cg.F90:116)
+template <Prec P, Prec RP>
+__global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, SpinorPtr rp, const CgScalars* cg) {
+  using R = typename SpinorView<P>::R;
+  using RR = typename SpinorView<RP>::R;
+  if (cg->done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  auto pv = sview<P>(pp, g.stride);
+  auto rv = sview<RP>(rp, g.stride);
+  Spinor<R> pl;
+  Spinor<RR> rl;
+  pv.load(i, pl);
+  rv.load(i, rl);
+  const R b = (R)cg->beta;
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) pl.c[s][c] = mkc((R)rl.c[s][c].x, (R)rl.c[s][c].y) + b * pl.c[s][c];
+  pv.store(i, pl);
+}
+
+void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  if (p == Prec::F64) k_cg_pupdate<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
+  else if (p == Prec::F32) k_cg_pupdate<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
+  else k_cg_pupdate<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
+}
+
+}  // namespace bqcdg

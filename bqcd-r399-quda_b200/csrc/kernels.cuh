@@ -1,0 +1,142 @@
+// kernels.cuh -- host-side declarations of the sm_100a kernels (launchers).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "bqcdg_internal.cuh"
+
+namespace bqcdg {
+
+// type-erased device pointers handed from the runtime to the launchers
+struct SpinorPtr {
+  void* v = nullptr;
+  float* norm = nullptr;  // F16 only
+};
+struct CloverPtr {
+  void* v = nullptr;
+  float* norm = nullptr;  // F16 only
+};
+
+// reduction scratch: per-block partials + arrival counter
+struct RedScratch {
+  double* partial = nullptr;  // [nval][maxblocks]
+  unsigned int* counter = nullptr;
+  int maxblocks = 0;
+};
+
+// scalars of a CG kept in device memory (no host round trip per iteration)
+struct CgScalars {
+  double rtr;       // |r|^2 after the latest update
+  double rtr_old;   // |r|^2 of the previous iteration
+  double paap;      // p.(A p) = |M p|^2
+  double alpha;
+  double beta;
+  double stop_rtr;  // converged when rtr <= stop_rtr
+  double ru_rtr;    // sloppy solver: request a reliable update when rtr < ru_rtr
+  int iter;         // iterations completed
+  int maxiter;
+  int done;         // 0 running, 1 converged, 2 reliable update requested, 3 maxiter
+  int pad;
+};
+
+struct OpParams {
+  double kappa;
+  double csw_kappa;
+  double h;
+  double rho;
+};
+
+constexpr int kBlock = 128;
+inline int nblocks(int n) { return (n + kBlock - 1) / kBlock; }
+
+// ---- stencil and clover operators (dslash.cu) ----
+void launch_dslash(Prec p, const Geom& g, int e, bool dag, SpinorPtr out, SpinorPtr in, const void* gauge,
+                   cudaStream_t s);
+// out = A in (mult_a); in-place allowed (mult_ao)
+void launch_clover_mult(Prec p, const Geom& g, SpinorPtr out, SpinorPtr in, CloverPtr a, cudaStream_t s);
+// in-place LDL solve with the B factors (F64 only)
+void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStream_t s);
+
+// first half of mtil / mtil_dag: out_o = [(1 -+ i h g5)] Ainv_oo D_oe in_e
+void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s);
+// second half: out_e = A_ee in_e + b D_eo t_o (+ h term for Wilson) + rho in_e;
+// optional |out|^2 reduction into *norm_out (device), and CG alpha update
+void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
+                       const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
+                       CgScalars* cg, cudaStream_t s);
+// CG-fused second half of mtil_dag: Ap = A_ee q + b D_eo t_o + rho q computed in
+// registers; x += alpha p, r -= alpha Ap, rtr = |r|^2.  Precision P for the
+// stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)
+void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
+                     const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
+                     cudaStream_t s);
+// p = r + beta p
+void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s);
+
+// ---- BLAS / conversions (blas.cu) ----
+// r = b - Ax (F64), copy r into p (precision pp); res2[0] = |r|^2, res2[1] = |b|^2
+void launch_residual(const Geom& g, double2* r, const double2* b, const double2* ax, Prec pp, SpinorPtr p,
+                     RedScratch red, double* res2, cudaStream_t s);
+// x = (1 + i h gamma_5) x (h_mult_b, h_mult.F90:51-82), F64
+void launch_h_mult_b(const Geom& g, double2* x, double h, cudaStream_t s);
+// halved inverse blocks from the LDL factors B (6 unit solves per block)
+void launch_ainv_from_b(const Geom& g, double2* ainv, const double2* b, cudaStream_t s);
+// generic copy/convert between spinor precisions
+void launch_spinor_convert(const Geom& g, Prec pout, SpinorPtr out, Prec pin, SpinorPtr in, cudaStream_t s);
+// x64 += xs (F32), xs = 0
+void launch_accum_x(const Geom& g, double2* x, float4* xs, cudaStream_t s);
+// |v|^2 of an F64 spinor -> *out (device)
+void launch_norm2(const Geom& g, const double2* v, RedScratch red, double* out, cudaStream_t s);
+// dot <a,b> real part of F64 spinors -> *out
+void launch_dot(const Geom& g, const double2* a, const double2* b, RedScratch red, double* out, cudaStream_t s);
+// y = a*x + y (F64)
+void launch_axpy(const Geom& g, double a, const double2* x, double2* y, cudaStream_t s);
+void launch_zero(const Geom& g, Prec p, SpinorPtr v, cudaStream_t s);
+
+// ---- layout conversions (convert.cu) ----
+// Fortran SPINCOL_FIELD complex(4,3,volh) <-> device F64 spinor
+void launch_spinor_from_fortran(const Geom& g, double2* dev, const double2* host_layout, cudaStream_t s);
+void launch_spinor_to_fortran(const Geom& g, double2* host_layout, const double2* dev, cudaStream_t s);
+// Fortran GAUGE_FIELD complex(3,3,volh,0:1,4) -> device F64 links (periodic);
+// flipped != 0: the input carries flip_bc's boundary sign, which is removed
+void launch_gauge_from_fortran(const Geom& g, double2* dev, const double2* host_layout, int flipped, cudaStream_t s);
+void launch_gauge_to_fortran(const Geom& g, double2* host_layout, const double2* dev, int flipped, cudaStream_t s);
+// Fortran CLOVER_FIELD_A/B (18,2,volh) for one parity -> device F64 [36][stride]
+void launch_clover_from_fortran(const Geom& g, double2* dev, const double2* host_layout, cudaStream_t s);
+void launch_clover_to_fortran(const Geom& g, double2* host_layout, const double2* dev, cudaStream_t s);
+// sloppy copies
+void launch_gauge_demote(const Geom& g, Prec p, void* out, const double2* in, cudaStream_t s);
+void launch_clover_demote(const Geom& g, Prec p, CloverPtr out, const double2* in, cudaStream_t s);
+// gauge-field SU(3) check: max |U U^+ - 1| and max |det U - 1| -> out[2]
+void launch_gauge_check(const Geom& g, const double2* gauge, RedScratch red, double* out, cudaStream_t s);
+
+// ---- forces (force.cu) ----
+// hopping force (dsf.F90:75-100): p(eo,mu) from a,b (even) and at,bt (odd)
+void launch_dsf_hop(const Geom& g, double* p, const double2* gauge, const double2* a, const double2* b,
+                    const double2* at, const double2* bt, double s, cudaStream_t st);
+// w planes of clover_bsa (6 planes x 9 complex per site) -> wbuf [6][9][stride]
+void launch_clover_bsa(const Geom& g, double2* w, const double2* b, const double2* a, cudaStream_t st);
+// w planes of clover_ts from the halved inverse blocks (clover_t_init + ts)
+void launch_clover_ts(const Geom& g, double2* w, const double2* ainv, cudaStream_t st);
+// clover_d: p(link) += contributions of the w planes of parity eo_w
+void launch_clover_d(const Geom& g, double* p, const double2* gauge, const double2* w, int eo_w, double s,
+                     cudaStream_t st);
+
+// ---- clover construction (clover_init.cu) ----
+// clover_init.F90 + clover_inv.F90 on device: A, Ainv, B for both parities
+void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, double2* a[2], double2* ainv[2],
+                        double2* b[2], cudaStream_t s);
+// 2 sum log det over the halved 1/D of B (clover_action.F90)
+void launch_clover_action(const Geom& g, const double2* b, RedScratch red, double* out, cudaStream_t s);
+
+// ---- seeded synthetic inputs (gauge_gen.cu) ----
+void ranf_powers(unsigned long long* pw);
+unsigned long long ranf_skip(unsigned long long seed, unsigned long long n);
+// ran_gauss_volh on the device: out[i*m + j] for draws 2(i m + j)+1, +2 from state s0
+void launch_ran_gauss(double2* out, int volh, int m, double var, unsigned long long s0, cudaStream_t s);
+void launch_u_normalize(double2* u_fortran, long long nlinks, cudaStream_t s);
+void launch_cold(double2* u_fortran, long long nlinks, cudaStream_t s);
+void launch_conf_relax(const Geom& g, double2* gauge, cudaStream_t s);
+void launch_plaquette(const Geom& g, const double2* gauge, RedScratch red, double* out, cudaStream_t s);
+
+}  // namespace bqcdg

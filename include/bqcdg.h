@@ -1,0 +1,207 @@
+/*
+ * bqcdg.h -- C ABI of the B200 (sm_100a) implementation of BQCD's fermion hot
+ * path: the even-odd preconditioned clover-Wilson operator, the M^+M
+ * conjugate-gradient solver and the pseudofermion force.
+ *
+ * Every entry point takes plain host pointers in BQCD's own Fortran layouts
+ * (defs.h:64-78), so BQCD's HMC driver can reach it through iso_c_binding:
+ *
+ *   SPINCOL_FIELD   complex(4,3,volh)        double[volh][3][4][2]   (one parity)
+ *   GAUGE_FIELD     complex(3,3,volh,0:1,4)  double[4][2][volh][3][3][2]
+ *   CLOVER_FIELD_A  type_clover_a(2,volh,0:1) double[2][volh][2][36]  (18 complex,
+ *   CLOVER_FIELD_B  type_clover_b(2,volh,0:1)  packed as clover/clover.h:28-82)
+ *   GENERATOR_FIELD real(8,volh,0:1,4)       double[4][2][volh][8]
+ *
+ * Site indices are BQCD's even/odd index i = ilex(x,y,z,t)/2 with parity
+ * (x+y+z+t) mod 2 (index.F90:26-76) on a single process (volh_tot = volh).
+ * Parities: 0 = EVEN, 1 = ODD.
+ *
+ * Boundary conditions: inside BQCD every fermion operation runs on links
+ * bracketed by flip_bc() (flip_bc.F90:97-121).  bqcdg_load_gauge() takes a
+ * flag saying whether the array passed carries that sign; the device keeps
+ * periodic links and applies the fermion boundary sign inside the kernels, so
+ * every operator below equals BQCD's on the flipped links in either case.
+ *
+ * All calls return BQCDG_OK (0) or a BQCDG_E* status; none aborts the
+ * process (the reference calls die(), misc.F90:28-37; a Fortran shim maps the
+ * status back).  A context is single-caller: like the reference's routines
+ * (which keep save-scratch, cg.F90:69) it is not reentrant.
+ */
+#ifndef BQCDG_H
+#define BQCDG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BQCDG_OK 0
+#define BQCDG_EINVAL 1       /* bad argument */
+#define BQCDG_ECUDA 2        /* CUDA runtime error (context is left usable) */
+#define BQCDG_ENOCONV 3      /* solver did not converge (cg.F90:121-124) */
+#define BQCDG_ENAN 4         /* residual became NaN/Inf */
+#define BQCDG_ENOGAUGE 5     /* no gauge field loaded */
+#define BQCDG_ENOCLOVER 6    /* clover term requested but not loaded/built */
+#define BQCDG_ENOMEM 7       /* device allocation failed */
+#define BQCDG_EUNSUPPORTED 8 /* e.g. h != 0 in the QUDA hook (invert_quda.F90:298-301) */
+#define BQCDG_ENOTSU3 9      /* links not SU(3): 12-real sloppy storage impossible */
+#define BQCDG_ENODEVICE 10   /* no CUDA device */
+
+typedef struct bqcdg_ctx bqcdg_ctx;
+
+/* the operator parameters of type(hmc_para) (modules/typedef_hmc.F90:32-44)
+ * that the hot path reads: M~ = A_ee - kappa^2/(1+h^2) D_eo A_oo^-1 D_oe
+ * (m_tilde.F90:43-77), W = M~ + rho (w_mult.F90:28-44) */
+typedef struct {
+  double kappa;
+  double csw_kappa; /* c_sw * kappa; 0 selects the Wilson operator */
+  double h;         /* external field of h_mult.F90 */
+  double rho;       /* Hasenbusch shift; 0 gives M~^+M~ (mtdagmt) */
+} bqcdg_params;
+
+/* type(type_cg_para) (cg.F90:30-34) */
+typedef struct {
+  float rest;   /* ABSOLUTE stop: |r|^2 <= rest, FP32 like the reference (cg.F90:111) */
+  int maxiter;
+  int log;      /* 2: no convergence is not an error (cg.F90:121) */
+} bqcdg_cg_para;
+
+/* precision of the inner CG iterations */
+#define BQCDG_PREC_DOUBLE 0 /* all FP64 */
+#define BQCDG_PREC_SINGLE 1 /* FP32 fields, FP64 reliable updates */
+#define BQCDG_PREC_HALF 2   /* int16 fields with norms, FP32 r/x, FP64 reliable updates */
+
+typedef struct {
+  int precision;      /* BQCDG_PREC_* */
+  int maxiter;
+  int relative;       /* 1: stop on |r|^2 <= tol^2 |b|^2, 0: |r|^2 <= tol (absolute) */
+  double tol;
+  double delta;       /* reliable update when |r| < delta * max|r| since the last one */
+  int check_true_residual; /* 1: recompute |b - A x|^2 in FP64 at the end */
+  int time_kernels;   /* 1: time every stencil launch with CUDA events */
+} bqcdg_solver_opts;
+
+typedef struct {
+  int niter;              /* inner iterations */
+  int reliable_updates;   /* FP64 residual recomputations */
+  double rtr;             /* final iterated |r|^2 */
+  double true_rtr;        /* final |b - A x|^2 in FP64 (if checked) */
+  double b2;              /* |b|^2 */
+  double seconds;         /* device time of the solve (CUDA events) */
+  double stencil_ms;      /* summed device time of the dominant stencil kernel */
+  int stencil_launches;   /* launches of that kernel */
+  int converged;
+  int kernel_launches;    /* all kernels this solve launched */
+} bqcdg_solve_info;
+
+/* ---- context ---------------------------------------------------------- */
+/* L: lattice extents (x,y,z,t), all even; bc: fermion boundary conditions
+ * (+1/-1, boundary_conditions_fermions of the input file) */
+int bqcdg_create(bqcdg_ctx **ctx, const int L[4], const int bc[4], int device);
+int bqcdg_destroy(bqcdg_ctx *ctx);
+const char *bqcdg_error_string(int status);
+/* volh of the context */
+int bqcdg_volh(const bqcdg_ctx *ctx);
+/* device memory held by the context, bytes */
+long long bqcdg_device_bytes(const bqcdg_ctx *ctx);
+
+/* ---- fields ----------------------------------------------------------- */
+/* conf%u; flipped = 1 if flip_bc() has been applied to the array.
+ * Replaces load_gauge_quda (invert_quda.F90:134). */
+int bqcdg_load_gauge(bqcdg_ctx *ctx, const double *u, int flipped);
+int bqcdg_get_gauge(bqcdg_ctx *ctx, double *u, int flipped);
+/* conf%a, conf%i, conf%b (both parities, any may be NULL).  Replaces
+ * load_clover_quda (invert_quda.F90:138). */
+int bqcdg_load_clover(bqcdg_ctx *ctx, const double *a, const double *ainv, const double *b);
+int bqcdg_get_clover(bqcdg_ctx *ctx, double *a, double *ainv, double *b);
+/* clover_init(a, i, b, u, csw_kappa) (clover/clover_init.F90:28) on the
+ * device, from the loaded links */
+int bqcdg_clover_init(bqcdg_ctx *ctx, double csw_kappa);
+/* clover_action(b(1,1,ODD)) (clover/clover_action.F90:29) */
+int bqcdg_clover_action(bqcdg_ctx *ctx, int eo, double *action);
+
+/* ---- operators on host spinor fields ----------------------------------- */
+/* d(e,o,out,in,u) / d_dag (d/D21.F90:29): out(parity e) = D_eo in(parity o) */
+int bqcdg_d(bqcdg_ctx *ctx, int e, int o, double *out, const double *in);
+int bqcdg_d_dag(bqcdg_ctx *ctx, int e, int o, double *out, const double *in);
+/* clover_mult_a(out, a(eo), in) (clover/clover_mult_a.F90:30) */
+int bqcdg_clover_mult_a(bqcdg_ctx *ctx, int eo, double *out, const double *in);
+/* clover_mult_ao(i(eo), x) (clover/clover_mult_ao.F90:30): x = A^-1 x */
+int bqcdg_clover_mult_ao(bqcdg_ctx *ctx, int eo, double *x);
+/* clover_mult_b(b(eo), x) (clover/clover_mult_b.F90:30): x = B^-1 x (LDL^+) */
+int bqcdg_clover_mult_b(bqcdg_ctx *ctx, int eo, double *x);
+/* mtil / mtil_dag (m_tilde.F90:43,80), mtdagmt (mtdagmt.F90:28),
+ * w_mult / w_mult_dag / w_dagger_w (w_mult.F90:28,46,64) */
+int bqcdg_mtil(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+int bqcdg_mtil_dag(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+int bqcdg_mtdagmt(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+int bqcdg_w_mult(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+int bqcdg_w_mult_dag(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+int bqcdg_w_dagger_w(bqcdg_ctx *ctx, double *out, const double *in, const bqcdg_params *p);
+
+/* ---- solvers ------------------------------------------------------------ */
+/* cg(matrix_mult, x, b, para, conf, iterations) (cg.F90:51) with
+ * matrix_mult = w_dagger_w (rho = p->rho) or mtdagmt (rho = 0): FP64 CG, x is
+ * the initial guess on input, absolute stop |r|^2 <= cgp->rest.  Returns
+ * BQCDG_ENOCONV on no convergence unless cgp->log == 2 (then BQCDG_OK). */
+int bqcdg_cg(bqcdg_ctx *ctx, double *x, const double *b, const bqcdg_params *p, const bqcdg_cg_para *cgp,
+             int *iterations, bqcdg_solve_info *info);
+/* quda_solver(matrix_mult, x, b, para, conf, iterations, rho)
+ * (invert_quda.F90:96): mixed-precision CG (int16 sloppy, FP64 reliable
+ * updates) to the same absolute criterion, then the FP64 true residual
+ * |b - W^+W x|^2 <= rest is re-checked on the device as invert_quda.F90:155-168
+ * does on the host.  Gauge and clover must be loaded (the reference uploads
+ * them on every call; here they stay resident until reloaded). */
+int bqcdg_quda_solver(bqcdg_ctx *ctx, double *x, const double *b, const bqcdg_params *p,
+                      const bqcdg_cg_para *cgp, int *iterations, bqcdg_solve_info *info);
+/* general entry: any precision, relative or absolute tolerance */
+int bqcdg_solve(bqcdg_ctx *ctx, double *x, const double *b, const bqcdg_params *p, const bqcdg_solver_opts *o,
+                bqcdg_solve_info *info);
+void bqcdg_solver_opts_default(bqcdg_solver_opts *o);
+
+/* ---- forces ------------------------------------------------------------- */
+/* dsf(p, conf, step, para, a, b) (dsf.F90:28): p += hopping + clover part of
+ * the pseudofermion force for the even fields a, b.  The gauge field must be
+ * loaded; the clover part needs conf%b/conf%i of the odd sites. */
+int bqcdg_dsf(bqcdg_ctx *ctx, double *p, double step, const bqcdg_params *par, const double *a, const double *b);
+/* clover_dsf(eo, p, b, a, s, u) (clover/clover_d.F90:78) */
+int bqcdg_clover_dsf(bqcdg_ctx *ctx, int eo, double *p, const double *b, const double *a, double s);
+/* clover_dsd(eo, p, b, s, u) (clover/clover_d.F90:40): determinant force */
+int bqcdg_clover_dsd(bqcdg_ctx *ctx, int eo, double *p, double s);
+
+/* ---- seeded synthetic inputs on the device ------------------------------ */
+/* the context's copy of the 48-bit LCG state of ranf.F90: ranset(seed, skip)
+ * (ranf.F90:87-121; seed 0 = the default seed) and ranget */
+int bqcdg_ranset(bqcdg_ctx *ctx, long long seed, long long skip);
+int bqcdg_ranget(bqcdg_ctx *ctx, long long *seed);
+/* conf_hot / conf_cold (conf.F90:172-217) into the context's links, drawing
+ * from the context's RNG stream exactly as ran_gauss_volh (ran.F90:28-110) */
+int bqcdg_conf_hot(bqcdg_ctx *ctx);
+int bqcdg_conf_cold(bqcdg_ctx *ctx);
+/* n sweeps of conf_relax (cooling.F90:131-193) on the context's links */
+int bqcdg_conf_relax(bqcdg_ctx *ctx, int n);
+/* sg(u) (action.F90:70-123): 6 V - sum Re Tr(plaquettes) / 3 */
+int bqcdg_sg(bqcdg_ctx *ctx, double *sg);
+
+/* ---- device-resident fields (benchmarks, repeated solves) ---------------- */
+/* spinor fields kept on the device between calls, addressed by handle */
+int bqcdg_field_create(bqcdg_ctx *ctx, int *handle);
+int bqcdg_field_upload(bqcdg_ctx *ctx, int handle, const double *host);
+int bqcdg_field_download(bqcdg_ctx *ctx, int handle, double *host);
+int bqcdg_field_destroy(bqcdg_ctx *ctx, int handle);
+/* fill a resident field with ran_gauss_volh(12, field, var, eo) from the
+ * context's RNG stream (var = 1/2 gives unit-variance complex entries) */
+int bqcdg_field_gauss(bqcdg_ctx *ctx, int handle, double var);
+/* solve with x, b resident (x: initial guess in, solution out) */
+int bqcdg_solve_dev(bqcdg_ctx *ctx, int hx, int hb, const bqcdg_params *p, const bqcdg_solver_opts *o,
+                    bqcdg_solve_info *info);
+/* out = (W^+W) in with both resident, repeated n times; *ms = average device
+ * time of one application (CUDA events on the context stream) */
+int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);
+/* average device time of one even-odd stencil pass (pass 1 of mtil: D_oe,
+ * Ainv_oo) at the given precision, n launches */
+int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precision, int n, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

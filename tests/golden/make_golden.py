@@ -1,0 +1,71 @@
+"""Regenerate the golden fixtures of the oracle tests from the reference's own
+test outputs (run in a checkout that has the reference sources mounted):
+
+  ranf_test.reference            -> ranf_test.json   (RNG known answers)
+  work/out.quick-test.reference  -> quick_test.json  (%it/%Favg/%Fmax/%fa records
+                                                      of one 4^4 HMC trajectory)
+
+Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def parse_ranf(path):
+    sections, cur = [], None
+    for line in open(path):
+        s = line.strip()
+        if not s:
+            continue
+        if s.endswith(":"):
+            cur = {"title": s, "records": []}
+            sections.append(cur)
+            continue
+        i, seed, x = s.split()
+        cur["records"].append([int(i), int(seed), x])
+    return sections
+
+
+def parse_quick(path):
+    out = {}
+    for line in open(path):
+        s = line.strip()
+        if s.startswith("%it"):
+            f = s.split()
+            out["it"] = {"traj": int(f[1]), "f1": int(f[2]), "f2": int(f[3])}
+        elif s.startswith("%Favg") or s.startswith("%Fmax"):
+            f = s.split()
+            out[f[0][1:]] = {"traj": int(f[1]), "values": [float(v) for v in f[2:6]],
+                             "names": ["F_gauge", "F_det", "F_F1", "F_F2"]}
+        elif s.startswith("%fa"):
+            f = s.split()
+            out["fa"] = {"traj": int(f[1]), "e": int(f[2]), "plaq_energy": float(f[3]), "exp_mdh": float(f[4]),
+                         "cg_calls": int(f[5]), "cg_it_tot": int(f[6]), "cg_it_max": int(f[7])}
+        elif s.startswith("Seed") and re.match(r"Seed\s+\d+$", s) and int(s.split()[1]) != 0:
+            out["final_seed"] = int(s.split()[1])
+        elif s.startswith("Program"):
+            out["program"] = s
+    out["input"] = {"lattice": [4, 4, 4, 4], "bc_fermions": [1, 1, 1, -1], "beta": 5.0, "kappa": 0.13,
+                    "csw": 2.3327, "h": 0.0, "hmc_model": "C", "hmc_rho": 0.1, "hmc_trajectory_length": 0.2,
+                    "hmc_steps": 10, "hmc_m_scale": 3, "start": "cold", "seed": "default", "solver_rest": 1e-5,
+                    "solver_maxiter": 1000, "solver_mre_vectors": 7, "force_accept": True}
+    return out
+
+
+def main(root):
+    ranf = parse_ranf(os.path.join(root, "ranf_test.reference"))
+    with open(os.path.join(HERE, "ranf_test.json"), "w") as f:
+        json.dump({"source": "ranf_test.reference (ranf_test.F90:26-93)", "sections": ranf}, f, indent=0)
+    quick = parse_quick(os.path.join(root, "work", "out.quick-test.reference"))
+    quick["source"] = "work/out.quick-test.reference:39-45,50 (work/input.quick-test)"
+    with open(os.path.join(HERE, "quick_test.json"), "w") as f:
+        json.dump(quick, f, indent=1)
+    print("wrote", len(ranf), "ranf sections and", sorted(quick))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

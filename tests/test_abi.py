@@ -1,0 +1,75 @@
+"""CPU checks of the drop-in boundary: the C ABI library exists, loads, exports
+every symbol include/bqcdg.h declares, and rejects bad calls without a GPU."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "bqcdg.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bqcdg_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def so():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bqbuild", os.path.join(ROOT, "bqcd-r399-quda_b200", "build.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m.build()
+
+
+def test_header_declares_the_reference_entry_points():
+    syms = declared_symbols()
+    for need in ("bqcdg_d", "bqcdg_d_dag", "bqcdg_clover_mult_a", "bqcdg_clover_mult_ao", "bqcdg_clover_mult_b",
+                 "bqcdg_mtil", "bqcdg_mtil_dag", "bqcdg_mtdagmt", "bqcdg_w_mult", "bqcdg_w_mult_dag",
+                 "bqcdg_w_dagger_w", "bqcdg_cg", "bqcdg_quda_solver", "bqcdg_dsf", "bqcdg_clover_dsf",
+                 "bqcdg_clover_dsd", "bqcdg_clover_init", "bqcdg_clover_action"):
+        assert need in syms
+
+
+def test_library_exports_every_declared_symbol(so):
+    lib = C.CDLL(so)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_error_strings_and_argument_checks(so):
+    lib = C.CDLL(so)
+    lib.bqcdg_error_string.restype = C.c_char_p
+    assert lib.bqcdg_error_string(0) == b"ok"
+    assert lib.bqcdg_error_string(3) == b"no convergence"
+    h = C.c_void_p()
+    L = (C.c_int * 4)(4, 4, 4, 4)
+    bad = (C.c_int * 4)(5, 4, 4, 4)          # odd extent: init_common.F90:67
+    bc = (C.c_int * 4)(1, 1, 1, -1)
+    badbc = (C.c_int * 4)(1, 1, 1, 0)
+    assert lib.bqcdg_create(C.byref(h), bad, bc, 0) == 1
+    assert lib.bqcdg_create(C.byref(h), L, badbc, 0) == 1
+    assert lib.bqcdg_create(None, L, bc, 0) == 1
+    assert lib.bqcdg_destroy(None) == 1
+    assert lib.bqcdg_d(None, 0, 1, None, None) == 1
+
+
+def test_no_device_is_reported_not_faulted(so):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = C.CDLL(so)
+    h = C.c_void_p()
+    rc = lib.bqcdg_create(C.byref(h), (C.c_int * 4)(4, 4, 4, 4), (C.c_int * 4)(1, 1, 1, -1), 0)
+    assert rc == 10  # BQCDG_ENODEVICE
+
+
+def test_python_mirror_fails_loudly_without_gpu(bq):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(bq.BqcdgError):
+        bq.Lattice((4, 4, 4, 4))
