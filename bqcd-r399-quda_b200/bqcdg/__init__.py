@@ -19,7 +19,7 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(HERE, "..", "lib", "libbqcdg.so")
+LIBPATH = os.environ.get("BQCDG_LIB", os.path.join(HERE, "..", "lib", "libbqcdg.so"))
 
 OK, EINVAL, ECUDA, ENOCONV, ENAN, ENOGAUGE, ENOCLOVER, ENOMEM, EUNSUPPORTED, ENOTSU3, ENODEVICE = range(11)
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
@@ -104,6 +104,8 @@ def _lib_handle():
         L.bqcdg_solve_dev.argtypes = [vp, i, i, P(Params), P(SolverOpts), P(SolveInfo)]
         L.bqcdg_mdagm_dev.argtypes = [vp, i, i, P(Params), i, i, P(C.c_double)]
         L.bqcdg_time_pass.argtypes = [vp, i, P(Params), i, i, P(C.c_double)]
+        L.bqcdg_solve_batch.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), P(SolverOpts), i,
+                                        P(SolveInfo)]
         L.bqcdg_ranset.argtypes = [vp, C.c_longlong, C.c_longlong]
         L.bqcdg_ranget.argtypes = [vp, P(C.c_longlong)]
         L.bqcdg_conf_hot.argtypes = [vp]
@@ -373,6 +375,20 @@ class Lattice:
         if st not in (OK, ENOCONV):
             _check(st, "solve_dev")
         return info
+
+    def solve_batch(self, hxs, hbs, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000,
+                    delta=0.1, block=0, rho=None):
+        """Batched mixed-precision solve of len(hxs) resident systems; block =
+        right-hand sides per launch (0: autotuned).  Returns the per-RHS infos."""
+        n = len(hxs)
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0)
+        infos = (SolveInfo * n)()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        st = lib().bqcdg_solve_batch(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm),
+                                     C.byref(o), block, infos)
+        if st not in (OK, ENOCONV):
+            _check(st, "solve_batch")
+        return list(infos)
 
     def mdagm_dev(self, hout, hin, para, precision, n, rho=None):
         ms = C.c_double()

@@ -44,10 +44,10 @@ __global__ void __launch_bounds__(kBlock) k_residual(Geom g, double2* r, const d
     Rv.store(i, rl);
     if (pp.v) bview<PP>(pp, g.stride).store(i, pl);
   }
-  block_reduce_store<2>(acc, red.partial, red.maxblocks);
-  if (last_block(red.counter)) {
+  block_reduce_store<2>(acc, red.partial, red.maxblocks, blockIdx.x);
+  if (last_block(red.counter, gridDim.x)) {
     double tot[2];
-    final_sum<2>(red.partial, red.maxblocks, tot);
+    final_sum<2>(red.partial, red.maxblocks, gridDim.x, tot);
     if (threadIdx.x == 0) {
       res2[0] = tot[0];
       res2[1] = tot[1];
@@ -76,6 +76,67 @@ __global__ void __launch_bounds__(kBlock) k_h_mult_b(Geom g, double2* x, double 
 
 void launch_h_mult_b(const Geom& g, double2* x, double h, cudaStream_t s) {
   k_h_mult_b<<<nblocks(g.volh), kBlock, 0, s>>>(g, x, h);
+}
+
+// real dot <r, p> of an F32 residual and a sloppy search direction
+template <Prec PP>
+__global__ void __launch_bounds__(kBlock) k_rdot(Geom g, SpinorPtr rp, SpinorPtr pp, RedScratch red, double* out) {
+  using RP = typename SpinorView<PP>::R;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (i < g.volh) {
+    Spinor<float> r;
+    Spinor<RP> p;
+    bview<Prec::F32>(rp, g.stride).load(i, r);
+    bview<PP>(pp, g.stride).load(i, p);
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        acc[0] += (double)r.c[s][c].x * (double)p.c[s][c].x + (double)r.c[s][c].y * (double)p.c[s][c].y;
+  }
+  block_reduce_store<1>(acc, red.partial, red.maxblocks, blockIdx.x);
+  if (last_block(red.counter, gridDim.x)) {
+    double tot[1];
+    final_sum<1>(red.partial, red.maxblocks, gridDim.x, tot);
+    if (threadIdx.x == 0) {
+      *out = tot[0];
+      *red.counter = 0;
+    }
+  }
+}
+
+// p = r + beta (p - rp r): the direction re-orthogonalised against the new
+// residual after a reliable update, then the CG step
+template <Prec PP>
+__global__ void __launch_bounds__(kBlock) k_p_reorth(Geom g, SpinorPtr pp, SpinorPtr rp, double rpc, double beta) {
+  using RP = typename SpinorView<PP>::R;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.volh) return;
+  Spinor<float> r;
+  Spinor<RP> p;
+  bview<Prec::F32>(rp, g.stride).load(i, r);
+  bview<PP>(pp, g.stride).load(i, p);
+  const RP a = (RP)(1.0 - beta * rpc), b = (RP)beta;
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) p.c[s][c] = a * mkc((RP)r.c[s][c].x, (RP)r.c[s][c].y) + b * p.c[s][c];
+  bview<PP>(pp, g.stride).store(i, p);
+}
+
+void launch_rdot(const Geom& g, SpinorPtr r32, Prec pp, SpinorPtr p, RedScratch red, double* out, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  if (pp == Prec::F64) k_rdot<Prec::F64><<<grid, kBlock, 0, s>>>(g, r32, p, red, out);
+  else if (pp == Prec::F32) k_rdot<Prec::F32><<<grid, kBlock, 0, s>>>(g, r32, p, red, out);
+  else k_rdot<Prec::F16><<<grid, kBlock, 0, s>>>(g, r32, p, red, out);
+}
+
+void launch_p_reorth(const Geom& g, Prec pp, SpinorPtr p, SpinorPtr r32, double rpc, double beta, cudaStream_t s) {
+  dim3 grid(nblocks(g.volh));
+  if (pp == Prec::F64) k_p_reorth<Prec::F64><<<grid, kBlock, 0, s>>>(g, p, r32, rpc, beta);
+  else if (pp == Prec::F32) k_p_reorth<Prec::F32><<<grid, kBlock, 0, s>>>(g, p, r32, rpc, beta);
+  else k_p_reorth<Prec::F16><<<grid, kBlock, 0, s>>>(g, p, r32, rpc, beta);
 }
 
 // halved A^-1 blocks (packed like conf%i) from the B factors, whose 1/D are
@@ -190,10 +251,10 @@ __global__ void __launch_bounds__(kBlock) k_dot(Geom g, const double2* a, const 
       acc[0] += x.x * y.x + x.y * y.y;
     }
   }
-  block_reduce_store<1>(acc, red.partial, red.maxblocks);
-  if (last_block(red.counter)) {
+  block_reduce_store<1>(acc, red.partial, red.maxblocks, blockIdx.x);
+  if (last_block(red.counter, gridDim.x)) {
     double tot[1];
-    final_sum<1>(red.partial, red.maxblocks, tot);
+    final_sum<1>(red.partial, red.maxblocks, gridDim.x, tot);
     if (threadIdx.x == 0) {
       *out = tot[0];
       *red.counter = 0;

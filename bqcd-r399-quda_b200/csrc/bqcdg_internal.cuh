@@ -111,6 +111,7 @@ struct Geom {
   int volh;
   int stride;      // padded per-component stride of every field
   int bcsign[4];   // fermion boundary sign per direction (+1 / -1)
+  int rec12;       // FP64 stencil links stored as 12 reals (columns 1,2)
 };
 
 struct Site {
@@ -296,9 +297,22 @@ struct GaugeView;
 template <>
 struct GaugeView<Prec::F64> {
   using R = double;
-  double2* v;  // [4][2][9][stride]
+  double2* v;  // [4][2][9][stride], or [4][2][6][stride] with rec12
   int stride;
+  int rec12 = 0;
   __device__ __forceinline__ void load(int mu, int eo, int i, Link<double>& u) const {
+    if (rec12) {
+      const double2* b = v + (size_t)((mu * 2 + eo) * 6) * stride + i;
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          double2 t = __ldg(b + (c * 3 + r) * stride);
+          u.m[r][c] = mkc(t.x, t.y);
+        }
+      reconstruct_col3(u);
+      return;
+    }
     const double2* b = v + (size_t)((mu * 2 + eo) * 9) * stride + i;
 #pragma unroll
     for (int c = 0; c < 3; c++)
@@ -637,10 +651,35 @@ __device__ __forceinline__ void h_mult_b(Spinor<R>& x, R h) {
 }
 
 // ---------------------------------------------------------------------------
-// deterministic block reductions
+// launch tiling: several right-hand sides share one launch.  CTA b serves RHS
+// b % nr and site block b / nr, so the nr CTAs reading the same links and
+// clover blocks are adjacent in the launch order: those fields come from HBM
+// once and from L2 for the other nr-1.  nr = 1 is the single-RHS launch.
+// ---------------------------------------------------------------------------
+constexpr int kMaxRhs = 16;
+constexpr int kRedVals = 4;  // reduction slots per RHS
+
+struct Tile {
+  int rhs;  // right-hand side of this CTA
+  int sb;   // site block
+  int nsb;  // site blocks per RHS
+  int i;    // site of this thread
+};
+__device__ __forceinline__ Tile tile(int nr) {
+  Tile t;
+  t.rhs = blockIdx.x % nr;
+  t.sb = blockIdx.x / nr;
+  t.nsb = gridDim.x / nr;
+  t.i = t.sb * blockDim.x + threadIdx.x;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// deterministic block reductions: partial[k * stride + sb] per value k, the
+// last of the nsb site blocks of one RHS to arrive sums them in block order
 // ---------------------------------------------------------------------------
 template <int N>
-__device__ __forceinline__ void block_reduce_store(double (&v)[N], double* partial, int nblocks_stride) {
+__device__ __forceinline__ void block_reduce_store(double (&v)[N], double* partial, int nblocks_stride, int sb) {
   __shared__ double red[N][32];
 #pragma unroll
   for (int k = 0; k < N; k++) {
@@ -662,34 +701,34 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[N], double* parti
       double x = lane < nw ? red[k][lane] : 0.0;
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
-      if (lane == 0) partial[k * nblocks_stride + blockIdx.x] = x;
+      if (lane == 0) partial[k * nblocks_stride + sb] = x;
     }
   }
 }
 
-// Called by every block after block_reduce_store; returns true in thread 0 of
-// the last block to arrive, which then sums the partials in block order.
-__device__ __forceinline__ bool last_block(unsigned int* counter) {
+// Called by every block after block_reduce_store; returns true in all threads
+// of the last of the nsb blocks to arrive, which then sums the partials.
+__device__ __forceinline__ bool last_block(unsigned int* counter, int nsb) {
   __shared__ bool is_last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     unsigned int t = atomicAdd(counter, 1u);
-    is_last = (t == gridDim.x - 1);
+    is_last = (t == (unsigned)nsb - 1u);
   }
   __syncthreads();
   return is_last;
 }
 
 template <int N>
-__device__ __forceinline__ void final_sum(const double* partial, int nblocks_stride, double (&out)[N]) {
+__device__ __forceinline__ void final_sum(const double* partial, int nblocks_stride, int nsb, double (&out)[N]) {
   // executed by the whole last block: warp-parallel fixed-order sum
   __shared__ double red[N][32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int k = 0; k < N; k++) {
     double x = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) x += __ldcg(partial + k * nblocks_stride + b);
+    for (int b = threadIdx.x; b < nsb; b += blockDim.x) x += __ldcg(partial + k * nblocks_stride + b);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
     if (lane == 0) red[k][warp] = x;

@@ -46,6 +46,10 @@ struct bqcdg_ctx {
   bool gauge_su3 = false;
   void* gauge_s[3] = {nullptr, nullptr, nullptr};  // by Prec
   bool gauge_s_ok[3] = {false, false, false};
+  // FP64 links of the even-odd operator stored as 12 reals (SU(3) links only)
+  double2* gauge64r = nullptr;
+  bool gauge64r_ok = false;
+  Geom g12{};  // g with rec12 set
 
   double2* A[2] = {nullptr, nullptr};
   double2* Ainv[2] = {nullptr, nullptr};
@@ -71,6 +75,24 @@ struct bqcdg_ctx {
   int next_handle = 1;
 
   unsigned long long seed = 48131768981101ull;  // ranf.F90:36 default seed
+
+  // batched sloppy vectors: nb right-hand sides per buffer, rsb bytes apart
+  struct Batch {
+    int cap = 0;
+    Prec prec = Prec::F64;
+    SpinorPtr p, t, q, rs, xs;
+  } batch;
+  int tuned_block[3] = {0, 0, 0};  // chosen RHS per launch, by precision
+
+  void release(void* p) {
+    if (!p) return;
+    for (size_t k = 0; k < allocations.size(); k++)
+      if (allocations[k] == p) {
+        allocations.erase(allocations.begin() + k);
+        break;
+      }
+    cudaFree(p);
+  }
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> kev;  // kernel-timing event pairs
@@ -196,7 +218,23 @@ int ensure_sloppy(bqcdg_ctx* c, Prec p, bool need_clover) {
   return BQCDG_OK;
 }
 
-const void* gauge_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? (const void*)c->gauge64 : c->gauge_s[(int)p]; }
+// FP64 operator links in 12-real form when the links are SU(3)
+int ensure_f64rec(bqcdg_ctx* c) {
+  if (c->gauge64r_ok || !c->gauge_su3) return BQCDG_OK;
+  if (!c->gauge64r) CK(c->alloc((void**)&c->gauge64r, (size_t)8 * 6 * c->g.stride * sizeof(double2)));
+  launch_gauge_demote(c->g, Prec::F64, c->gauge64r, c->gauge64, c->stream);
+  CKL();
+  c->gauge64r_ok = true;
+  return BQCDG_OK;
+}
+bool use_rec(bqcdg_ctx* c, Prec p) {
+  return p == Prec::F64 && c->gauge_su3 && ensure_f64rec(c) == BQCDG_OK && c->gauge64r_ok;
+}
+const Geom& geom_of(bqcdg_ctx* c, Prec p) { return use_rec(c, p) ? c->g12 : c->g; }
+const void* gauge_of(bqcdg_ctx* c, Prec p) {
+  if (p == Prec::F64) return use_rec(c, p) ? (const void*)c->gauge64r : (const void*)c->gauge64;
+  return c->gauge_s[(int)p];
+}
 CloverPtr aee_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? C(c->A[0]) : c->aee_s[(int)p]; }
 CloverPtr ainv_of(bqcdg_ctx* c, Prec p) { return p == Prec::F64 ? C(c->Ainv[1]) : c->ainv_oo_s[(int)p]; }
 
@@ -210,8 +248,9 @@ int check_op(bqcdg_ctx* c, const bqcdg_params* p) {
 // out_e = M~ in_e  (dag: M~^+), with rho for W; t_o scratch (odd)
 void apply_mtil(bqcdg_ctx* c, Prec p, bool dag, SpinorPtr out, SpinorPtr in, SpinorPtr t, const OpParams& op,
                 double* norm_out, CgScalars* cg) {
-  launch_mtil_pass1(p, c->g, dag, t, in, gauge_of(c, p), ainv_of(c, p), op, cg, c->stream);
-  launch_mtil_pass2(p, c->g, dag, out, t, in, gauge_of(c, p), aee_of(c, p), op, c->red, norm_out, cg, c->stream);
+  const Geom& g = geom_of(c, p);
+  launch_mtil_pass1(p, g, dag, t, in, gauge_of(c, p), ainv_of(c, p), op, cg, c->stream);
+  launch_mtil_pass2(p, g, dag, out, t, in, gauge_of(c, p), aee_of(c, p), op, c->red, norm_out, cg, c->stream);
 }
 
 // out = (W^+ W) in in precision p; scratch t (odd), q (even)
@@ -257,6 +296,8 @@ struct KernelTimer {
     pending.clear();
   }
 };
+
+constexpr int kStalled = 100;  // internal: the sloppy precision stopped converging
 
 // Core CG on device-resident x, b (F64, device layout).  Solves (W^+W) x = b.
 //   sloppy == F64: plain FP64 CG (cg.F90)
@@ -315,8 +356,11 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   h.rtr_old = rtr;
   h.stop_rtr = stop_rtr;
   h.maxiter = maxiter;
-  h.ru_rtr = sloppy == Prec::F64 ? -1.0 : delta * delta * rtr;
-  double maxr2 = rtr;
+  h.delta2 = sloppy == Prec::F64 ? 0.0 : delta * delta;
+  h.maxr2 = rtr;
+  double best = rtr;  // smallest true |r|^2 so far
+  int stall = 0;      // reliable updates in a row without progress
+  bool stalled = false;
   int ru = 0;
   int nl = 5 + (sloppy != Prec::F64 ? 2 : 0);  // kernels launched so far
   bool converged = false;
@@ -326,19 +370,20 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   { int st_ = write_cg(c); if (st_) return st_; }
 
   int batch = 4;
+  const Geom& gs = geom_of(c, sloppy);  // stencil geometry (12-real FP64 links when SU(3))
   while (!h.done) {
     nl += 5 * batch;
     for (int k = 0; k < batch; k++) {
       // pass 1 (timed), pass 2 (+|M~p|^2 -> alpha), pass 3, pass 4 (+x,r update, |r|^2), p update
       kt.begin();
-      launch_mtil_pass1(sloppy, g, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
+      launch_mtil_pass1(sloppy, gs, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
       kt.end();
-      launch_mtil_pass2(sloppy, g, false, q, t, p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
+      launch_mtil_pass2(sloppy, gs, false, q, t, p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
                         c->dcg, c->stream);
       kt.begin();
-      launch_mtil_pass1(sloppy, g, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
+      launch_mtil_pass1(sloppy, gs, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
       kt.end();
-      launch_cg_pass4(sloppy, g, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
+      launch_cg_pass4(sloppy, gs, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
                       c->stream);
       launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream);
     }
@@ -366,14 +411,24 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     if (!(rtrue == rtrue)) { h.done = 4; break; }
     if (rtrue <= stop_rtr) { h.rtr = rtrue; converged = true; h.done = 1; break; }
     if (h.done == 3) { h.rtr = rtrue; break; }
-    // continue from the true residual: p = r + beta p with beta = |r|^2 / |r_old|^2
-    maxr2 = rtrue;
+    // progress check: the sloppy precision has run out when the true residual
+    // stops falling (or grows) over several reliable updates
+    if (rtrue < 0.5 * best) { best = rtrue; stall = 0; }
+    else if (++stall >= 5 || rtrue > 1e4 * best) { h.rtr = rtrue; stalled = true; break; }
+    // continue from the true residual with p re-orthogonalised against it:
+    // p = r + beta (p - (<r,p>/|r|^2) r), beta = |r|^2 / |r_old|^2
+    launch_rdot(g, rs, sloppy, p, c->red, c->dres, c->stream);
+    CKL();
+    CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double rpc = c->hres[0] / rtrue;
     h.beta = rtrue / h.rtr_old;
     h.rtr = rtrue;
-    h.ru_rtr = delta * delta * maxr2;
+    h.maxr2 = rtrue;
     h.done = 0;
     { int st_ = write_cg(c); if (st_) return st_; }
-    launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream);
+    launch_p_reorth(g, sloppy, p, rs, rpc, h.beta, c->stream);
+    nl += 2;
     CKL();
   }
   CK(cudaEventRecord(c->ev1, c->stream));
@@ -389,7 +444,39 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   info->stencil_ms = kt.ms;
   info->stencil_launches = kt.launches;
   if (h.done == 4) return BQCDG_ENAN;
+  if (stalled) return kStalled;
   return BQCDG_OK;
+}
+
+// cg_core with precision escalation: when the sloppy iterations stop making
+// progress on the true residual (ill-conditioned systems can exhaust int16
+// accuracy), continue from the current x with FP32, and then FP64, sloppy
+// fields.  Statistics add up over the stages.
+int cg_robust(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec sloppy, int maxiter, double stop_rtr,
+              double delta, bool min_one_iter, bool time_kernels, bqcdg_solve_info* info) {
+  bqcdg_solve_info sum;
+  std::memset(&sum, 0, sizeof(sum));
+  Prec cur = sloppy;
+  for (;;) {
+    bqcdg_solve_info one;
+    std::memset(&one, 0, sizeof(one));
+    int st = cg_core(c, x, b, op, cur, maxiter - sum.niter, stop_rtr, delta, min_one_iter && sum.niter == 0,
+                     time_kernels, &one);
+    if (sum.niter == 0) sum.b2 = one.b2;
+    sum.niter += one.niter;
+    sum.reliable_updates += one.reliable_updates;
+    sum.kernel_launches += one.kernel_launches;
+    sum.seconds += one.seconds;
+    sum.stencil_ms += one.stencil_ms;
+    sum.stencil_launches += one.stencil_launches;
+    sum.rtr = one.rtr;
+    sum.converged = one.converged;
+    if (st != kStalled || cur == Prec::F64) {
+      *info = sum;
+      return st == kStalled ? BQCDG_OK : st;
+    }
+    cur = cur == Prec::F16 ? Prec::F32 : Prec::F64;
+  }
 }
 
 int true_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, double* rtr) {
@@ -405,6 +492,220 @@ int true_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, doub
 }
 
 Prec prec_of(int p) { return p == BQCDG_PREC_DOUBLE ? Prec::F64 : (p == BQCDG_PREC_SINGLE ? Prec::F32 : Prec::F16); }
+
+// one buffer of nb fields of precision p, rsb bytes apart
+int alloc_batched(bqcdg_ctx* c, Prec p, int nb, SpinorPtr& out) {
+  out = SpinorPtr{};
+  out.rsb = (long long)c->spin_bytes(p);
+  CK(c->alloc(&out.v, (size_t)out.rsb * nb));
+  CK(cudaMemsetAsync(out.v, 0, (size_t)out.rsb * nb, c->stream));
+  if (p == Prec::F16) {
+    out.rsnb = (long long)sizeof(float) * c->g.stride;
+    CK(c->alloc((void**)&out.norm, (size_t)out.rsnb * nb));
+    CK(cudaMemsetAsync(out.norm, 0, (size_t)out.rsnb * nb, c->stream));
+  }
+  return BQCDG_OK;
+}
+
+int ensure_batch(bqcdg_ctx* c, Prec p, int nb) {
+  auto& B = c->batch;
+  if (B.cap >= nb && B.prec == p) return BQCDG_OK;
+  for (SpinorPtr* s : {&B.p, &B.t, &B.q, &B.rs, &B.xs}) {
+    c->release(s->v);
+    c->release(s->norm);
+    *s = SpinorPtr{};
+  }
+  B.cap = 0;
+  int st;
+  if ((st = alloc_batched(c, p, nb, B.p)) || (st = alloc_batched(c, p, nb, B.t)) ||
+      (st = alloc_batched(c, p, nb, B.q)) || (st = alloc_batched(c, Prec::F32, nb, B.rs)) ||
+      (st = alloc_batched(c, Prec::F32, nb, B.xs)))
+    return st;
+  B.cap = nb;
+  B.prec = p;
+  return BQCDG_OK;
+}
+
+// r = b - A x in FP64 for one right-hand side, r copied into rs (F32);
+// returns |r|^2 and |b|^2
+int fp64_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, SpinorPtr rs, double* r2, double* b2) {
+  double2 *r = c->sp64(0), *ax = c->sp64(1);
+  apply_mdagm(c, Prec::F64, S(ax), S(x), S(c->sp64(2)), S(c->sp64(3)), op);
+  launch_residual(c->g, r, b, ax, Prec::F32, rs, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *r2 = c->hres[0];
+  if (b2) *b2 = c->hres[1];
+  return BQCDG_OK;
+}
+
+// Batched mixed-precision CG over nb right-hand sides: the five kernels of a
+// sloppy iteration each serve all nb (CTAs rhs-fastest), every right-hand
+// side has its own scalars, stops and FP64 reliable updates, and a converged
+// or paused one costs its CTAs an early return only.
+int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op, Prec sloppy, int maxiter,
+             const double* stop, double delta, bqcdg_solve_info* info) {
+  const Geom& g = c->g;
+  int st = ensure_sloppy(c, sloppy, op.csw_kappa != 0.0);
+  if (st) return st;
+  if ((st = ensure_batch(c, sloppy, nb))) return st;
+  auto& B = c->batch;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  std::vector<int> ru(nb, 0), fin(nb, 0), conv(nb, 0), nl(nb, 0), stall(nb, 0), stalled(nb, 0);
+  std::vector<double> best(nb, 0.0);
+  for (int k = 0; k < nb; k++) {
+    double r2, b2;
+    if ((st = fp64_residual(c, x[k], b[k], op, rhs_of(B.rs, k), &r2, &b2))) return st;
+    launch_spinor_convert(g, sloppy, rhs_of(B.p, k), Prec::F32, rhs_of(B.rs, k), c->stream);
+    launch_zero(g, Prec::F32, rhs_of(B.xs, k), c->stream);
+    CKL();
+    CgScalars& h = c->hcg[k];
+    std::memset(&h, 0, sizeof(h));
+    h.rtr = h.rtr_old = r2;
+    h.stop_rtr = stop[k];
+    h.maxiter = maxiter;
+    h.delta2 = delta * delta;
+    h.maxr2 = r2;
+    best[k] = r2;
+    info[k].b2 = b2;
+    if (!(r2 == r2)) { h.done = 4; fin[k] = 1; }
+    else if (r2 <= stop[k]) { h.done = 1; fin[k] = 1; conv[k] = 1; }
+    else if (maxiter <= 0) { h.done = 3; fin[k] = 1; }
+  }
+  CK(cudaMemcpyAsync(c->dcg, c->hcg, sizeof(CgScalars) * nb, cudaMemcpyHostToDevice, c->stream));
+  int batch = 4, launches = 0;
+  auto running = [&]() {
+    for (int k = 0; k < nb; k++)
+      if (!fin[k]) return true;
+    return false;
+  };
+  while (running()) {
+    for (int it = 0; it < batch; it++) {
+      launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
+                        nb);
+      launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
+                        c->dcg, c->stream, nb);
+      launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
+                        nb);
+      launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
+                      c->dcg, c->stream, nb);
+      launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
+    }
+    launches += 5 * batch;
+    CKL();
+    CK(cudaMemcpyAsync(c->hcg, c->dcg, sizeof(CgScalars) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (batch < 16) batch *= 2;
+    std::vector<int> resume;
+    for (int k = 0; k < nb; k++) {
+      CgScalars& h = c->hcg[k];
+      if (fin[k] || h.done == 0) continue;
+      if (h.done == 4) { fin[k] = 1; continue; }
+      // reliable update of right-hand side k: x += x_s, r = b - A x in FP64
+      launch_accum_x(g, x[k], (float4*)rhs_of(B.xs, k).v, c->stream);
+      double rt;
+      if ((st = fp64_residual(c, x[k], b[k], op, rhs_of(B.rs, k), &rt, nullptr))) return st;
+      ru[k]++;
+      launches += 7;
+      if (!(rt == rt)) { h.done = 4; fin[k] = 1; continue; }
+      if (rt <= stop[k]) { h.rtr = rt; h.done = 1; fin[k] = 1; conv[k] = 1; continue; }
+      if (h.done == 3) { h.rtr = rt; fin[k] = 1; continue; }
+      if (rt < 0.5 * best[k]) { best[k] = rt; stall[k] = 0; }
+      else if (++stall[k] >= 5 || rt > 1e4 * best[k]) {
+        // retire it here; it is finished below at a higher sloppy precision
+        h.rtr = rt;
+        h.done = 1;
+        fin[k] = 1;
+        stalled[k] = 1;
+        continue;
+      }
+      h.beta = rt / h.rtr_old;
+      h.rtr = rt;
+      h.maxr2 = rt;
+      h.done = 0;
+      resume.push_back(k);
+    }
+    CK(cudaMemcpyAsync(c->dcg, c->hcg, sizeof(CgScalars) * nb, cudaMemcpyHostToDevice, c->stream));
+    for (int k : resume) {
+      // p = r + beta (p - (<r,p>/|r|^2) r)
+      launch_rdot(g, rhs_of(B.rs, k), sloppy, rhs_of(B.p, k), c->red, c->dres, c->stream);
+      CKL();
+      CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      launch_p_reorth(g, sloppy, rhs_of(B.p, k), rhs_of(B.rs, k), c->hres[0] / c->hcg[k].rtr, c->hcg[k].beta,
+                      c->stream);
+      launches += 2;
+    }
+    CKL();
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  bool nan = false;
+  std::vector<CgScalars> hs(c->hcg, c->hcg + nb);
+  for (int k = 0; k < nb; k++) {
+    info[k].seconds = ms * 1e-3;
+    info[k].niter = hs[k].iter;
+    info[k].reliable_updates = ru[k];
+    info[k].rtr = hs[k].rtr;
+    info[k].converged = conv[k];
+    info[k].kernel_launches = launches;
+    nan = nan || hs[k].done == 4;
+  }
+  // right-hand sides whose int16 iterations stalled: finish alone from the
+  // current x with FP32 (then FP64) sloppy fields
+  for (int k = 0; k < nb; k++) {
+    if (!stalled[k]) continue;
+    bqcdg_solve_info more;
+    std::memset(&more, 0, sizeof(more));
+    int st2 = cg_robust(c, x[k], b[k], op, sloppy == Prec::F16 ? Prec::F32 : Prec::F64,
+                        maxiter - info[k].niter, stop[k], delta, false, false, &more);
+    if (st2) return st2;
+    info[k].niter += more.niter;
+    info[k].reliable_updates += more.reliable_updates;
+    info[k].seconds += more.seconds;
+    info[k].rtr = more.rtr;
+    info[k].converged = more.converged;
+  }
+  return nan ? BQCDG_ENAN : BQCDG_OK;
+}
+
+// RHS per launch for a batch: the per-RHS time of the first stencil pass,
+// timed for 1, 4, 8 and 16 right-hand sides on the resident fields
+int tune_block(bqcdg_ctx* c, Prec p, const OpParams& op, int nmax, int* best) {
+  const int cand[4] = {1, 4, 8, 16};
+  int cap = 1;
+  for (int k = 0; k < 4; k++)
+    if (cand[k] <= nmax) cap = cand[k];
+  int st = ensure_sloppy(c, p, op.csw_kappa != 0.0);
+  if (st) return st;
+  if ((st = ensure_batch(c, p, cap))) return st;
+  double bestt = 1e300;
+  *best = 1;
+  for (int k = 0; k < 4 && cand[k] <= cap; k++) {
+    int nb = cand[k];
+    for (int w = 0; w < 2; w++)
+      launch_mtil_pass1(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
+                        c->stream, nb);
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < 3; r++)
+      launch_mtil_pass1(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
+                        c->stream, nb);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CKL();
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    double per_rhs = ms / (3.0 * nb);
+    if (per_rhs < bestt * 0.98) {
+      bestt = per_rhs;
+      *best = nb;
+    }
+  }
+  return BQCDG_OK;
+}
 
 }  // namespace
 
@@ -450,19 +751,23 @@ int bqcdg_create(bqcdg_ctx** out, const int L[4], const int bc[4], int device) {
   c->g.Lxh = L[0] / 2;
   c->g.volh = (int)(vol / 2);
   c->g.stride = (c->g.volh + 63) / 64 * 64;
+  c->g.rec12 = 0;
+  c->g12 = c->g;
+  c->g12.rec12 = 1;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   c->staging_bytes = (size_t)c->g.volh * 72 * sizeof(double2);
   if (e == cudaSuccess) e = c->alloc((void**)&c->staging, c->staging_bytes);
   c->red.maxblocks = nblocks(c->g.volh);
-  if (e == cudaSuccess) e = c->alloc((void**)&c->red.partial, sizeof(double) * 4 * c->red.maxblocks);
-  if (e == cudaSuccess) e = c->alloc((void**)&c->red.counter, sizeof(unsigned int) * 4);
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->red.counter, 0, sizeof(unsigned int) * 4, c->stream);
+  if (e == cudaSuccess)
+    e = c->alloc((void**)&c->red.partial, sizeof(double) * kRedVals * kMaxRhs * c->red.maxblocks);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->red.counter, sizeof(unsigned int) * kMaxRhs);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->red.counter, 0, sizeof(unsigned int) * kMaxRhs, c->stream);
   if (e == cudaSuccess) e = c->alloc((void**)&c->dres, sizeof(double) * 16);
-  if (e == cudaSuccess) e = c->alloc((void**)&c->dcg, sizeof(CgScalars));
+  if (e == cudaSuccess) e = c->alloc((void**)&c->dcg, sizeof(CgScalars) * kMaxRhs);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hres, sizeof(double) * 16);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hcg, sizeof(CgScalars));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hcg, sizeof(CgScalars) * kMaxRhs);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     bqcdg_destroy(c);
@@ -504,6 +809,7 @@ int bqcdg_load_gauge(bqcdg_ctx* c, const double* u, int flipped) {
   c->gauge_su3 = c->hres[0] < 1e-10 && c->hres[1] < 1e-10;
   c->have_gauge = true;
   for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  c->gauge64r_ok = false;
   return BQCDG_OK;
 }
 
@@ -703,7 +1009,7 @@ static int solve_resident(bqcdg_ctx* c, double2* x, double2* b, const bqcdg_para
   } else {
     stop = o->tol;
   }
-  int st = cg_core(c, x, b, op, sl, o->maxiter, stop, o->delta, false, o->time_kernels != 0, info);
+  int st = cg_robust(c, x, b, op, sl, o->maxiter, stop, o->delta, false, o->time_kernels != 0, info);
   if (st) return st;
   info->kernel_launches += o->relative ? 1 : 0;
   if (o->check_true_residual) {
@@ -773,7 +1079,7 @@ int bqcdg_quda_solver(bqcdg_ctx* c, double* x, const double* b, const bqcdg_para
   OpParams op = op_of(p, true);
   // QUDA stops on |r| < sqrt(rest) (L2 absolute, invert_quda.F90:143,342)
   Prec sl = c->gauge_su3 ? Prec::F16 : Prec::F64;
-  st = cg_core(c, dx, db, op, sl, cgp->maxiter, (double)cgp->rest, 0.1, false, false, info);
+  st = cg_robust(c, dx, db, op, sl, cgp->maxiter, (double)cgp->rest, 0.1, false, false, info);
   if (st) return st;
   // host-side check of invert_quda.F90:155-168, done in FP64 on the device
   if ((st = true_residual(c, dx, db, op, &info->true_rtr))) return st;
@@ -967,6 +1273,7 @@ static int gauge_finish(bqcdg_ctx* c) {
   c->gauge_su3 = c->hres[0] < 1e-10 && c->hres[1] < 1e-10;
   c->have_gauge = true;
   for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  c->gauge64r_ok = false;
   return BQCDG_OK;
 }
 
@@ -1001,6 +1308,7 @@ int bqcdg_conf_relax(bqcdg_ctx* c, int n) {
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
+  c->gauge64r_ok = false;
   return BQCDG_OK;
 }
 
@@ -1023,6 +1331,57 @@ int bqcdg_solve_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const b
   if (!o || !field(c, hx) || !field(c, hb)) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   return solve_resident(c, field(c, hx), field(c, hb), p, o, info);
+}
+
+int bqcdg_solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
+                      const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!o || !hx || !hb || !infos || nrhs <= 0 || block < 0 || block > kMaxRhs) return BQCDG_EINVAL;
+  for (int k = 0; k < nrhs; k++)
+    if (!field(c, hx[k]) || !field(c, hb[k])) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  OpParams op = op_of(p, true);
+  Prec sl = prec_of(o->precision);
+  if (sl == Prec::F64) return BQCDG_EUNSUPPORTED;  // the batched path is the mixed-precision one
+  std::memset(infos, 0, sizeof(bqcdg_solve_info) * nrhs);
+  if (block == 0) {
+    int k = (int)sl;
+    if (!c->tuned_block[k] && (st = tune_block(c, sl, op, kMaxRhs, &c->tuned_block[k]))) return st;
+    block = c->tuned_block[k];
+  }
+  std::vector<double> stop(nrhs);
+  for (int k = 0; k < nrhs; k++) {
+    if (o->relative) {
+      launch_norm2(c->g, field(c, hb[k]), c->red, c->dres, c->stream);
+      CKL();
+      CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      stop[k] = o->tol * o->tol * c->hres[0];
+    } else {
+      stop[k] = o->tol;
+    }
+  }
+  bool all_conv = true;
+  for (int k0 = 0; k0 < nrhs; k0 += block) {
+    int nb = nrhs - k0 < block ? nrhs - k0 : block;
+    std::vector<double2*> xs(nb), bs(nb);
+    for (int k = 0; k < nb; k++) {
+      xs[k] = field(c, hx[k0 + k]);
+      bs[k] = field(c, hb[k0 + k]);
+    }
+    st = cg_batch(c, xs.data(), bs.data(), nb, op, sl, o->maxiter, stop.data() + k0, o->delta, infos + k0);
+    if (st) return st;
+    for (int k = 0; k < nb; k++) {
+      bqcdg_solve_info& in = infos[k0 + k];
+      if (o->check_true_residual) {
+        if ((st = true_residual(c, xs[k], bs[k], op, &in.true_rtr))) return st;
+        in.converged = in.true_rtr <= stop[k0 + k] ? 1 : 0;
+      }
+      all_conv = all_conv && in.converged;
+    }
+  }
+  return all_conv ? BQCDG_OK : BQCDG_ENOCONV;
 }
 
 int bqcdg_mdagm_dev(bqcdg_ctx* c, int hout, int hin, const bqcdg_params* p, int precision, int n, double* ms) {
@@ -1077,7 +1436,7 @@ int bqcdg_time_pass(bqcdg_ctx* c, int hin, const bqcdg_params* p, int precision,
   }
   CK(cudaEventRecord(c->ev0, c->stream));
   for (int k = 0; k < n; k++)
-    launch_mtil_pass1(pr, c->g, false, t, in, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream);
+    launch_mtil_pass1(pr, geom_of(c, pr), false, t, in, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream);
   CK(cudaEventRecord(c->ev1, c->stream));
   CKL();
   CK(cudaStreamSynchronize(c->stream));

@@ -204,10 +204,10 @@ __global__ void __launch_bounds__(kBlock) k_clover_action(Geom g, const double2*
     }
     acc[0] = log(d1 * d2);
   }
-  block_reduce_store<1>(acc, red.partial, red.maxblocks);
-  if (last_block(red.counter)) {
+  block_reduce_store<1>(acc, red.partial, red.maxblocks, blockIdx.x);
+  if (last_block(red.counter, gridDim.x)) {
     double tot[1];
-    final_sum<1>(red.partial, red.maxblocks, tot);
+    final_sum<1>(red.partial, red.maxblocks, gridDim.x, tot);
     if (threadIdx.x == 0) {
       *out = 2.0 * tot[0];
       *red.counter = 0;

@@ -125,9 +125,20 @@ __global__ void __launch_bounds__(kBlock) k_gauge_demote16(Geom g, short4* out, 
     dst[k * g.stride] = make_short4(q16(a.x), q16(a.y), q16(b.x), q16(b.y));
   }
 }
+// FP64 12-real copy: the first six entries (columns 1, 2) of every link
+__global__ void __launch_bounds__(kBlock) k_gauge_compress64(Geom g, double2* out, const double2* in) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int me = blockIdx.y;
+  if (i >= g.volh) return;
+#pragma unroll
+  for (int k = 0; k < 6; k++)
+    out[((size_t)me * 6 + k) * g.stride + i] = in[((size_t)me * 9 + k) * g.stride + i];
+}
+
 void launch_gauge_demote(const Geom& g, Prec p, void* out, const double2* in, cudaStream_t s) {
   dim3 grid(nblocks(g.volh), 8);
-  if (p == Prec::F32) k_gauge_demote32<<<grid, kBlock, 0, s>>>(g, (float4*)out, in);
+  if (p == Prec::F64) k_gauge_compress64<<<grid, kBlock, 0, s>>>(g, (double2*)out, in);
+  else if (p == Prec::F32) k_gauge_demote32<<<grid, kBlock, 0, s>>>(g, (float4*)out, in);
   else k_gauge_demote16<<<grid, kBlock, 0, s>>>(g, (short4*)out, in);
 }
 

@@ -11,9 +11,15 @@
 
 namespace bqcdg {
 
+// Resident CTAs per SM requested from the register allocator.  The reduced-
+// precision stencils move few bytes per thread, so latency hiding needs more
+// warps in flight than the FP64 ones (whose per-thread loads are 2-4x larger).
+#ifndef BQCDG_SLOPPY_MIN_BLOCKS
+#define BQCDG_SLOPPY_MIN_BLOCKS 8
+#endif
 template <Prec P>
-struct Views {
-  using R = typename SpinorView<P>::R;
+struct Occ {
+  static constexpr int min_blocks = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS;
 };
 
 template <Prec P>
@@ -32,18 +38,18 @@ __device__ __forceinline__ SpinorView<Prec::F16> sview<Prec::F16>(SpinorPtr p, i
 }
 
 template <Prec P>
-__device__ __forceinline__ GaugeView<P> gview(const void* p, int stride);
+__device__ __forceinline__ GaugeView<P> gview(const void* p, const Geom& g);
 template <>
-__device__ __forceinline__ GaugeView<Prec::F64> gview<Prec::F64>(const void* p, int stride) {
-  return GaugeView<Prec::F64>{(double2*)p, stride};
+__device__ __forceinline__ GaugeView<Prec::F64> gview<Prec::F64>(const void* p, const Geom& g) {
+  return GaugeView<Prec::F64>{(double2*)p, g.stride, g.rec12};
 }
 template <>
-__device__ __forceinline__ GaugeView<Prec::F32> gview<Prec::F32>(const void* p, int stride) {
-  return GaugeView<Prec::F32>{(float4*)p, stride};
+__device__ __forceinline__ GaugeView<Prec::F32> gview<Prec::F32>(const void* p, const Geom& g) {
+  return GaugeView<Prec::F32>{(float4*)p, g.stride};
 }
 template <>
-__device__ __forceinline__ GaugeView<Prec::F16> gview<Prec::F16>(const void* p, int stride) {
-  return GaugeView<Prec::F16>{(short4*)p, stride};
+__device__ __forceinline__ GaugeView<Prec::F16> gview<Prec::F16>(const void* p, const Geom& g) {
+  return GaugeView<Prec::F16>{(short4*)p, g.stride};
 }
 
 template <Prec P>
@@ -71,7 +77,7 @@ __global__ void __launch_bounds__(kBlock) k_dslash(Geom g, int e, SpinorPtr outp
   if (i >= g.volh) return;
   auto in = sview<P>(inp, g.stride);
   auto out = sview<P>(outp, g.stride);
-  auto U = gview<P>(gauge, g.stride);
+  auto U = gview<P>(gauge, g);
   Site st = site_coords(g, i, e);
   Spinor<R> b;
   wilson_hop<P, P, DAG>(g, e, i, st, in, U, b);
@@ -184,15 +190,17 @@ void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStrea
 //   t_o = Ainv_oo D_oe in_e, then (1 - i h g5) t_o for mtil, (1 + i h g5) for mtil_dag
 // ---------------------------------------------------------------------------
 template <Prec P, bool DAG>
-__global__ void __launch_bounds__(kBlock) k_pass1(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge,
-                                                  CloverPtr ainv, int has_clover, double hval, const CgScalars* cg) {
+__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge,
+                                                  CloverPtr ainv, int has_clover, double hval, const CgScalars* cg,
+                                                  int nr) {
   using R = typename SpinorView<P>::R;
-  if (cg && cg->done) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const Tile tl = tile(nr);
+  if (cg && cg[tl.rhs].done) return;  // retired right-hand side
+  const int i = tl.i;
   if (i >= g.volh) return;
-  auto in = sview<P>(inp, g.stride);
-  auto out = sview<P>(outp, g.stride);
-  auto U = gview<P>(gauge, g.stride);
+  auto in = sview<P>(rhs_of(inp, tl.rhs), g.stride);
+  auto out = sview<P>(rhs_of(outp, tl.rhs), g.stride);
+  auto U = gview<P>(gauge, g);
   Site st = site_coords(g, i, 1);
   Spinor<R> b;
   wilson_hop<P, P, DAG>(g, 1, i, st, in, U, b);
@@ -206,11 +214,11 @@ __global__ void __launch_bounds__(kBlock) k_pass1(Geom g, SpinorPtr outp, Spinor
 }
 
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
-                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s) {
-  dim3 grid(nblocks(g.volh));
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr) {
+  dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double hv = dag ? op.h : -op.h;
-#define P1(PP, D) k_pass1<PP, D><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg)
+#define P1(PP, D) k_pass1<PP, D><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr)
   if (p == Prec::F64) { if (dag) P1(Prec::F64, true); else P1(Prec::F64, false); }
   else if (p == Prec::F32) { if (dag) P1(Prec::F32, true); else P1(Prec::F32, false); }
   else { if (dag) P1(Prec::F16, true); else P1(Prec::F16, false); }
@@ -263,19 +271,20 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
 }
 
 template <Prec P, bool DAG, bool REDUCE>
-__global__ void __launch_bounds__(kBlock) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
+__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
                                                   const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                                                   double hval, double rho, RedScratch red, double* norm_out,
-                                                  CgScalars* cg) {
+                                                  CgScalars* cg, int nr) {
   using R = typename SpinorView<P>::R;
-  if (cg && cg->done) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const Tile tl = tile(nr);
+  if (cg && cg[tl.rhs].done) return;  // retired right-hand side
+  const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
-    auto t = sview<P>(tp, g.stride);
-    auto xin = sview<P>(xp, g.stride);
-    auto out = sview<P>(outp, g.stride);
-    auto U = gview<P>(gauge, g.stride);
+    auto t = sview<P>(rhs_of(tp, tl.rhs), g.stride);
+    auto xin = sview<P>(rhs_of(xp, tl.rhs), g.stride);
+    auto out = sview<P>(rhs_of(outp, tl.rhs), g.stride);
+    auto U = gview<P>(gauge, g);
     Spinor<R> o, x;
     pass2_core<P, DAG>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o, x);
     out.store(i, o);
@@ -287,17 +296,19 @@ __global__ void __launch_bounds__(kBlock) k_pass2(Geom g, SpinorPtr outp, Spinor
     }
   }
   if (REDUCE) {
-    block_reduce_store<1>(acc, red.partial, red.maxblocks);
-    if (last_block(red.counter)) {
+    double* part = red.partial + (size_t)tl.rhs * kRedVals * red.maxblocks;
+    block_reduce_store<1>(acc, part, red.maxblocks, tl.sb);
+    if (last_block(red.counter + tl.rhs, tl.nsb)) {
       double tot[1];
-      final_sum<1>(red.partial, red.maxblocks, tot);
+      final_sum<1>(part, red.maxblocks, tl.nsb, tot);
       if (threadIdx.x == 0) {
-        if (norm_out) *norm_out = tot[0];
+        if (norm_out) norm_out[tl.rhs] = tot[0];
         if (cg) {
-          cg->paap = tot[0];
-          cg->alpha = cg->rtr / tot[0];
+          CgScalars* c = cg + tl.rhs;
+          c->paap = tot[0];
+          c->alpha = c->rtr / tot[0];
         }
-        *red.counter = 0;
+        red.counter[tl.rhs] = 0;
       }
     }
   }
@@ -305,14 +316,15 @@ __global__ void __launch_bounds__(kBlock) k_pass2(Geom g, SpinorPtr outp, Spinor
 
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s) {
-  dim3 grid(nblocks(g.volh));
+                       CgScalars* cg, cudaStream_t s, int nr) {
+  dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = dag ? -op.h : op.h;
   bool reduce = norm_out != nullptr || cg != nullptr;
-#define P2(PP, D, RR) \
-  k_pass2<PP, D, RR><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, norm_out, cg)
+#define P2(PP, D, RR)                                                                                                \
+  k_pass2<PP, D, RR><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, norm_out, \
+                                             cg, nr)
 #define P2R(PP, D) \
   if (reduce) P2(PP, D, true); else P2(PP, D, false);
   if (p == Prec::F64) { if (dag) { P2R(Prec::F64, true) } else { P2R(Prec::F64, false) } }
@@ -337,24 +349,26 @@ struct XR<Prec::F32> {
 };
 
 template <Prec P, Prec XP>
-__global__ void __launch_bounds__(kBlock) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
+__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
-                                                     RedScratch red, CgScalars* cg) {
+                                                     RedScratch red, CgScalars* cgs, int nr) {
   using R = typename SpinorView<P>::R;
   using RX = typename SpinorView<XP>::R;
-  if (cg->done) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const Tile tl = tile(nr);
+  CgScalars* cg = cgs + tl.rhs;
+  if (cg->done) return;  // retired right-hand side
+  const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
-    auto t = sview<P>(tp, g.stride);
-    auto q = sview<P>(qp, g.stride);
-    auto U = gview<P>(gauge, g.stride);
+    auto t = sview<P>(rhs_of(tp, tl.rhs), g.stride);
+    auto q = sview<P>(rhs_of(qp, tl.rhs), g.stride);
+    auto U = gview<P>(gauge, g);
     Spinor<R> ap, qq;
     pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap, qq);
-    auto pv = sview<P>(pp, g.stride);
-    auto xv = sview<XP>(xp, g.stride);
-    auto rv = sview<XP>(rp, g.stride);
+    auto pv = sview<P>(rhs_of(pp, tl.rhs), g.stride);
+    auto xv = sview<XP>(rhs_of(xp, tl.rhs), g.stride);
+    auto rv = sview<XP>(rhs_of(rp, tl.rhs), g.stride);
     Spinor<R> pl;
     pv.load(i, pl);
     Spinor<RX> xl, rl;
@@ -374,53 +388,58 @@ __global__ void __launch_bounds__(kBlock) k_cg_pass4(Geom g, SpinorPtr tp, Spino
     xv.store(i, xl);
     rv.store(i, rl);
   }
-  block_reduce_store<1>(acc, red.partial, red.maxblocks);
-  if (last_block(red.counter)) {
+  double* part = red.partial + (size_t)tl.rhs * kRedVals * red.maxblocks;
+  block_reduce_store<1>(acc, part, red.maxblocks, tl.sb);
+  if (last_block(red.counter + tl.rhs, tl.nsb)) {
     double tot[1];
-    final_sum<1>(red.partial, red.maxblocks, tot);
+    final_sum<1>(part, red.maxblocks, tl.nsb, tot);
     if (threadIdx.x == 0) {
       double rtr = tot[0];
       cg->iter += 1;
       cg->rtr_old = cg->rtr;
       cg->rtr = rtr;
       cg->beta = rtr / cg->rtr_old;
+      if (rtr > cg->maxr2) cg->maxr2 = rtr;
       if (!(rtr == rtr)) cg->done = 4;  // NaN: stop, reported as an error
       else if (rtr <= cg->stop_rtr) cg->done = 1;
       else if (cg->iter >= cg->maxiter) cg->done = 3;
-      else if (rtr < cg->ru_rtr) cg->done = 2;
-      *red.counter = 0;
+      else if (rtr < cg->delta2 * cg->maxr2) cg->done = 2;  // reliable update (|r| < delta max|r|)
+      red.counter[tl.rhs] = 0;
     }
   }
 }
 
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s) {
-  dim3 grid(nblocks(g.volh));
+                     cudaStream_t s, int nr) {
+  dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = -op.h;  // mtil_dag
   if (p == Prec::F64)
     k_cg_pass4<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg);
+                                                             x, r, red, cg, nr);
   else if (p == Prec::F32)
     k_cg_pass4<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg);
+                                                             x, r, red, cg, nr);
   else
     k_cg_pass4<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg);
+                                                             x, r, red, cg, nr);
 }
 
 // p = r + beta p   (sc_xpby, cg.F90:116)
 template <Prec P, Prec RP>
-__global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, SpinorPtr rp, const CgScalars* cg) {
+__global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, SpinorPtr rp, const CgScalars* cgs,
+                                                       int nr) {
   using R = typename SpinorView<P>::R;
   using RR = typename SpinorView<RP>::R;
+  const Tile tl = tile(nr);
+  const CgScalars* cg = cgs + tl.rhs;
   if (cg->done) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = tl.i;
   if (i >= g.volh) return;
-  auto pv = sview<P>(pp, g.stride);
-  auto rv = sview<RP>(rp, g.stride);
+  auto pv = sview<P>(rhs_of(pp, tl.rhs), g.stride);
+  auto rv = sview<RP>(rhs_of(rp, tl.rhs), g.stride);
   Spinor<R> pl;
   Spinor<RR> rl;
   pv.load(i, pl);
@@ -433,11 +452,11 @@ __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, Spi
   pv.store(i, pl);
 }
 
-void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s) {
-  dim3 grid(nblocks(g.volh));
-  if (p == Prec::F64) k_cg_pupdate<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
-  else if (p == Prec::F32) k_cg_pupdate<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
-  else k_cg_pupdate<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg);
+void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s, int nr) {
+  dim3 grid(nblocks(g.volh) * nr);
+  if (p == Prec::F64) k_cg_pupdate<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
+  else if (p == Prec::F32) k_cg_pupdate<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
+  else k_cg_pupdate<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
 }
 
 }  // namespace bqcdg

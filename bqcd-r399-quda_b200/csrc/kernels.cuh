@@ -10,7 +10,19 @@ namespace bqcdg {
 struct SpinorPtr {
   void* v = nullptr;
   float* norm = nullptr;  // F16 only
+  long long rsb = 0;      // bytes from one RHS's field to the next (batched launches)
+  long long rsnb = 0;     // same for the norms
 };
+
+// the field of right-hand side r in a batched SpinorPtr
+__host__ __device__ __forceinline__ SpinorPtr rhs_of(SpinorPtr p, int r) {
+  SpinorPtr q = p;
+  if (r) {
+    q.v = (char*)p.v + r * p.rsb;
+    if (p.norm) q.norm = (float*)((char*)p.norm + r * p.rsnb);
+  }
+  return q;
+}
 struct CloverPtr {
   void* v = nullptr;
   float* norm = nullptr;  // F16 only
@@ -31,11 +43,13 @@ struct CgScalars {
   double alpha;
   double beta;
   double stop_rtr;  // converged when rtr <= stop_rtr
-  double ru_rtr;    // sloppy solver: request a reliable update when rtr < ru_rtr
+  double ru_rtr;    // unused (kept for layout); see delta2/maxr2
   int iter;         // iterations completed
   int maxiter;
-  int done;         // 0 running, 1 converged, 2 reliable update requested, 3 maxiter
+  int done;         // 0 running, 1 converged, 2 reliable update requested, 3 maxiter, 4 NaN
   int pad;
+  double delta2;    // sloppy solver: reliable update when rtr < delta2 * maxr2 (0: never)
+  double maxr2;     // largest |r|^2 since the last reliable update
 };
 
 struct OpParams {
@@ -57,26 +71,32 @@ void launch_clover_mult(Prec p, const Geom& g, SpinorPtr out, SpinorPtr in, Clov
 void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStream_t s);
 
 // first half of mtil / mtil_dag: out_o = [(1 -+ i h g5)] Ainv_oo D_oe in_e
+// (nr > 1: nr right-hand sides in one launch, fields at SpinorPtr::rsb strides,
+//  cg / norm_out arrays of nr entries; retired RHS return at once)
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
-                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s);
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr = 1);
 // second half: out_e = A_ee in_e + b D_eo t_o (+ h term for Wilson) + rho in_e;
 // optional |out|^2 reduction into *norm_out (device), and CG alpha update
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s);
+                       CgScalars* cg, cudaStream_t s, int nr = 1);
 // CG-fused second half of mtil_dag: Ap = A_ee q + b D_eo t_o + rho q computed in
 // registers; x += alpha p, r -= alpha Ap, rtr = |r|^2.  Precision P for the
 // stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s);
+                     cudaStream_t s, int nr = 1);
 // p = r + beta p
-void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s);
+void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,
+                       int nr = 1);
 
 // ---- BLAS / conversions (blas.cu) ----
 // r = b - Ax (F64), copy r into p (precision pp); res2[0] = |r|^2, res2[1] = |b|^2
 void launch_residual(const Geom& g, double2* r, const double2* b, const double2* ax, Prec pp, SpinorPtr p,
                      RedScratch red, double* res2, cudaStream_t s);
+// reliable-update helpers: *out = <r32, p> (real), then p = r + beta (p - rpc r)
+void launch_rdot(const Geom& g, SpinorPtr r32, Prec pp, SpinorPtr p, RedScratch red, double* out, cudaStream_t s);
+void launch_p_reorth(const Geom& g, Prec pp, SpinorPtr p, SpinorPtr r32, double rpc, double beta, cudaStream_t s);
 // x = (1 + i h gamma_5) x (h_mult_b, h_mult.F90:51-82), F64
 void launch_h_mult_b(const Geom& g, double2* x, double h, cudaStream_t s);
 // halved inverse blocks from the LDL factors B (6 unit solves per block)

@@ -194,6 +194,14 @@ int bqcdg_field_gauss(bqcdg_ctx *ctx, int handle, double var);
 /* solve with x, b resident (x: initial guess in, solution out) */
 int bqcdg_solve_dev(bqcdg_ctx *ctx, int hx, int hb, const bqcdg_params *p, const bqcdg_solver_opts *o,
                     bqcdg_solve_info *info);
+/* batched solve of nrhs systems (W^+W) x_k = b_k sharing one operator: every
+ * sloppy iteration of all unconverged right-hand sides runs in the same five
+ * launches, so each link and clover block is read from HBM once per site for
+ * the whole batch; converged right-hand sides retire inside the kernels and
+ * each gets its own FP64 reliable updates.  block = right-hand sides per
+ * launch (1..16; 0 = choose by timing 1, 4, 8 and 16).  infos: nrhs entries. */
+int bqcdg_solve_batch(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
+                      const bqcdg_solver_opts *o, int block, bqcdg_solve_info *infos);
 /* out = (W^+W) in with both resident, repeated n times; *ms = average device
  * time of one application (CUDA events on the context stream) */
 int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);

@@ -1,0 +1,83 @@
+"""The pseudofermion force against central finite differences of the action.
+
+S_f1 = phi^+ (W^+W)^-1 phi with W = M~ + rho (the clover operator on the
+flipped links; the clover blocks are rebuilt on the device from each perturbed
+gauge field).  dsf (dsf.F90:28) adds p -= step * dS/domega_j for
+U -> exp(i omega_j lambda_j) U (hmc_u.F90:53-60), so along a direction h
+(h_j per link) the derivative is  dS/deps = -(p_new - p_old).h / step.
+Checked along 16 random su(3) directions with eps = 1e-5 to 1e-7 relative.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def gell_mann():
+    lam = np.zeros((8, 3, 3), complex)
+    lam[0][0, 1] = lam[0][1, 0] = 1
+    lam[1][0, 1], lam[1][1, 0] = -1j, 1j
+    lam[2][0, 0], lam[2][1, 1] = 1, -1
+    lam[3][0, 2] = lam[3][2, 0] = 1
+    lam[4][0, 2], lam[4][2, 0] = -1j, 1j
+    lam[5][1, 2] = lam[5][2, 1] = 1
+    lam[6][1, 2], lam[6][2, 1] = -1j, 1j
+    lam[7] = np.diag([1, 1, -2]) / np.sqrt(3)
+    return lam
+
+
+def perturb(oracle, u, h, eps):
+    """U -> exp(i eps h_j lambda_j) U on every link -- the update of hmc_u.F90
+    (gen2u, su3.F90:28, whose generators are the Gell-Mann matrices of
+    im_tr_j).  The exponential is taken exactly from the eigen-decomposition
+    of the Hermitian H = h.lambda: gen2u's closed form loses accuracy (and is
+    undefined at h = 0) for arguments as small as eps = 1e-5.  Links are
+    stored [col][row], so a stored block is the transposed matrix."""
+    H = np.einsum("...j,jab->...ab", h, gell_mann())
+    w, V = np.linalg.eigh(H)
+    E = (V * np.exp(1j * eps * w)[..., None, :]) @ np.conj(np.swapaxes(V, -1, -2))
+    M = np.swapaxes(u, -1, -2)
+    return np.swapaxes(E @ M, -1, -2).copy()
+
+
+def action(lat, g, oracle, u, phi, para, csw_kappa):
+    uf = g.flip_bc(u.copy())
+    lat.load_gauge(uf, flipped=True)
+    lat.clover_init(csw_kappa)
+    x, info = lat.solve(np.zeros_like(phi), phi, para, precision=0, tol=1e-13, rho=para.rho)
+    assert info.converged
+    wx = lat.w_mult(x, para)
+    return float(np.vdot(wx, wx).real)
+
+
+@pytest.mark.parametrize("csw", [0.0, 1.9192])
+def test_dsf_matches_finite_differences(oracle, bq, csw):
+    L = (4, 4, 4, 4)
+    g = oracle.Geom(L, (1, 1, 1, -1))
+    oracle.ranset(2024)
+    u = g.hot()
+    g.relax(u, 2)
+    kappa, rho = 0.12, 0.1
+    para = bq.HmcPara(kappa=kappa, csw=csw, rho=rho)
+    phi = g.gauss_spinor(0)
+    rng = np.random.default_rng(7)
+    with bq.Lattice(L, (1, 1, 1, -1)) as lat:
+        # force at U: a = (W^+W)^-1 phi, b = W a  (dsf1.F90:64-71)
+        uf = g.flip_bc(u.copy())
+        lat.load_gauge(uf, flipped=True)
+        lat.clover_init(csw * kappa)
+        a, info = lat.solve(np.zeros_like(phi), phi, para, precision=0, tol=1e-13)
+        b = lat.w_mult(a, para)
+        step = 1.0
+        p0 = np.zeros((4, 2, lat.volh, 8))
+        dS = -lat.dsf(p0.copy(), step, para, a, b) / step          # dS/domega_j per link
+        eps = 1e-5
+        errs = []
+        for _ in range(16):
+            h = rng.standard_normal((4, 2, lat.volh, 8))
+            sp = action(lat, g, oracle, perturb(oracle, u, h, eps), phi, para, csw * kappa)
+            sm = action(lat, g, oracle, perturb(oracle, u, h, -eps), phi, para, csw * kappa)
+            fd = (sp - sm) / (2 * eps)
+            an = float(np.sum(dS * h))
+            errs.append(abs(fd - an) / abs(an))
+        assert max(errs) < 1e-7, errs

@@ -59,6 +59,22 @@ def test_cg_no_convergence_semantics(setup, bq):
     assert it == 3 and info.converged == 0
 
 
+@pytest.mark.parametrize("prec", [0, 2])
+def test_nan_input_reports_status_and_context_survives(setup, bq, prec):
+    """A NaN planted on the host in b ends the solve with BQCDG_ENAN (no
+    fault, no hang), and the same context then solves a clean system."""
+    g, lat = setup["g"], setup["lat"]
+    b = g.gauss_spinor(0)
+    bad = b.copy()
+    bad[3, 1, 2] = np.nan
+    para = bq.HmcPara(kappa=setup["kappa"], csw=setup["csw"])
+    with pytest.raises(bq.BqcdgError) as e:
+        lat.solve(np.zeros_like(b), bad, para, precision=prec, tol=1e-10, relative=False)
+    assert e.value.status == bq.ENAN
+    x, info = lat.solve(np.zeros_like(b), b, para, precision=prec, tol=1e-10)
+    assert info.converged == 1
+
+
 @pytest.mark.parametrize("rho", [0.0, 0.1])
 def test_quda_solver_mixed_precision(setup, bq, rho):
     """The hook's replacement: int16 sloppy iterations + FP64 reliable updates
