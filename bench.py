@@ -35,6 +35,14 @@ for _p in (ROOT, PKG):
 
 METRIC = "M†M CG time-to-1e-10 at 32^3x64: mixed vs FP64 (1 B200); D-slash HBM GB/s"
 KAPPA, CSW, COOL = 0.13, 1.9192, 10
+# The 32^3x64 configuration asks for hot-start links smoothed "by 10 steps of
+# seeded cooling to plaquette ~0.55".  One sweep of BQCD's conf_relax (a full
+# Cabibbo-Marinari minimisation) already takes a hot start to 0.61, and ten
+# sweeps reach 0.98, a nearly free field on which kappa = 0.13 is beyond the
+# critical hopping parameter (FP64 CG then needs ~30,000 iterations).  The
+# benchmark therefore cools until the plaquette first reaches the stated
+# value; --cool N forces N sweeps.
+PLAQ_TARGET = 0.55
 
 
 def peaks():
@@ -142,11 +150,21 @@ def allmax(pg, v, local):
     return float(t.item())
 
 
-def build_system(bq, L, device, seed_skip):
+def build_system(bq, L, device, seed_skip, cool):
+    """Hot start, then conf_relax sweeps.  cool < 0: sweep until the plaquette
+    (<Re Tr P>/3) first reaches PLAQ_TARGET, at most COOL sweeps."""
     lat = bq.Lattice(L, (1, 1, 1, -1), device=device)
     lat.ranset(0)
     lat.conf_hot()
-    lat.conf_relax(COOL)
+    sweeps = 0
+    if cool >= 0:
+        lat.conf_relax(cool)
+        sweeps = cool
+    else:
+        while sweeps < COOL and 1.0 - lat.plaq_energy() < PLAQ_TARGET:
+            lat.conf_relax(1)
+            sweeps += 1
+    lat.sweeps = sweeps
     lat.clover_init(CSW * KAPPA)
     lat.ranset(0, seed_skip)
     hb = lat.field()
@@ -175,7 +193,7 @@ def run_ours(args):
     world, rank, local, pg = dist_init()
     L = tuple(int(x) for x in args.lattice.split(","))
     peak, peak_kind = peaks()
-    lat, hb, hx = build_system(bq, L, local, 1000003 * rank)
+    lat, hb, hx = build_system(bq, L, local, 1000003 * rank, args.cool)
     para = bq.HmcPara(kappa=KAPPA, csw=CSW)
     zero = np.zeros((lat.volh, 3, 4), np.complex128)
     plaq = 1.0 - lat.plaq_energy()
@@ -250,7 +268,8 @@ def run_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64 (int16/f32 sloppy iterations)",
-            "data": "synthetic: device hot start (BQCD ranf, default seed) + %d cooling sweeps, Gaussian b" % COOL,
+            "data": "synthetic: device hot start (BQCD ranf, default seed) + %d conf_relax cooling sweep(s) "
+                    "(plaquette %.4f), Gaussian b" % (lat.sweeps, plaq),
             "config": {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
                                    % ("x".join(map(str, L)), KAPPA, CSW),
                        "lattice": list(L), "volh": lat.volh, "plaquette": round(plaq, 6),
@@ -314,7 +333,13 @@ def run_reference(args):
     g = O.Geom(L, (1, 1, 1, -1))
     O.ranset(0)
     u = g.hot()
-    g.relax(u, COOL)
+    if args.cool >= 0:
+        g.relax(u, args.cool)
+    else:
+        sweeps = 0
+        while sweeps < COOL and 1.0 - g.sg(u) / (6.0 * 2 * g.volh) < PLAQ_TARGET:
+            g.relax(u, 1)
+            sweeps += 1
     clov = g.clover_init(u, CSW * KAPPA)
     g.flip_bc(u)
     O.ranset(0)
@@ -368,6 +393,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--cool", type=int, default=-1,
+                    help="conf_relax sweeps; -1: until the plaquette reaches %.2f" % PLAQ_TARGET)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

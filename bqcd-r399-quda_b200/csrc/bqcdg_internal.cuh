@@ -190,6 +190,15 @@ struct SpinorView<Prec::F64> {
 #pragma unroll
       for (int sp = 0; sp < 4; sp++) v[(c * 4 + sp) * stride + i] = make_double2(s.c[sp][c].x, s.c[sp][c].y);
   }
+  // values up to a common factor (1 here); the int16 view defers its scale
+  __device__ __forceinline__ void load_raw(int i, Spinor<double>& s, double& sc) const {
+    load(i, s);
+    sc = 1.0;
+  }
+  __device__ __forceinline__ void load_pair_raw(int i, int s0, cx<double> h[2][3], double& sc) const {
+    load_pair(i, s0, h);
+    sc = 1.0;
+  }
 };
 
 template <>
@@ -223,11 +232,32 @@ struct SpinorView<Prec::F32> {
                                       s.c[k1 & 3][k1 >> 2].y);
     }
   }
+  __device__ __forceinline__ void load_raw(int i, Spinor<float>& s, float& sc) const {
+    load(i, s);
+    sc = 1.0f;
+  }
+  __device__ __forceinline__ void load_pair_raw(int i, int s0, cx<float> h[2][3], float& sc) const {
+    load_pair(i, s0, h);
+    sc = 1.0f;
+  }
 };
 
-__device__ __forceinline__ float q2f(short q, float scale) { return (float)q * scale; }
-__device__ __forceinline__ short f2q(float v, float inv) {
-  return (short)__float2int_rn(v * inv);
+
+// int16 <-> float without the quarter-rate I2F/F2I conversions.  Load: bias
+// the pair to unsigned (q + 32768), splice each half into the mantissa of
+// 2^23 with a byte permute and subtract 2^23 + 2^15 -- exact for every int16.
+__device__ __forceinline__ float2 s16x2_to_f2(unsigned w) {
+  const unsigned u = w ^ 0x80008000u;
+  const float lo = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7610)) - 8421376.0f;
+  const float hi = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7632)) - 8421376.0f;
+  return make_float2(lo, hi);
+}
+// Store: a + 1.5*2^23 rounds a (|a| <= 32767) to the nearest integer and
+// leaves it, in two's complement, in the low 16 bits of the mantissa.
+__device__ __forceinline__ unsigned f2_to_s16x2(float a, float b, float scale) {
+  const unsigned ia = __float_as_uint(fmaf(a, scale, 12582912.0f));
+  const unsigned ib = __float_as_uint(fmaf(b, scale, 12582912.0f));
+  return __byte_perm(ia, ib, 0x5410);
 }
 
 template <>
@@ -237,28 +267,47 @@ struct SpinorView<Prec::F16> {
   float* norm;  // [stride]
   int stride;
   __device__ __forceinline__ void load(int i, Spinor<float>& s) const {
-    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
+    float sc;
+    load_raw(i, s, sc);
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      int4 t = __ldg(v + k * stride + i);
-      const short* q = reinterpret_cast<const short*>(&t);
+    for (int a = 0; a < 4; a++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        int comp = 4 * k + j;  // colour k, spin j
-        s.c[comp & 3][comp >> 2] = mkc(q2f(q[2 * j], scale), q2f(q[2 * j + 1], scale));
-      }
-    }
+      for (int b = 0; b < 3; b++) s.c[a][b] = sc * s.c[a][b];
   }
   __device__ __forceinline__ void load_pair(int i, int s0, cx<float> h[2][3]) const {
-    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
+    float sc;
+    load_pair_raw(i, s0, h, sc);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      // colour c occupies int4 number c; spins s0,s0+1 are its halves
+      h[0][c] = sc * h[0][c];
+      h[1][c] = sc * h[1][c];
+    }
+  }
+  // raw int16 values as floats; the true value is raw * sc (the stencil
+  // applies sc once, after the linear projection and transport).  int4
+  // number k holds colour k, spins 0..3, one complex per 32-bit word.
+  __device__ __forceinline__ void load_raw(int i, Spinor<float>& s, float& sc) const {
+    sc = __ldg(norm + i) * (1.0f / 32767.0f);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int4 t = __ldg(v + k * stride + i);
+      const float2 a = s16x2_to_f2(t.x), b = s16x2_to_f2(t.y), c = s16x2_to_f2(t.z), d = s16x2_to_f2(t.w);
+      s.c[0][k] = mkc(a.x, a.y);
+      s.c[1][k] = mkc(b.x, b.y);
+      s.c[2][k] = mkc(c.x, c.y);
+      s.c[3][k] = mkc(d.x, d.y);
+    }
+  }
+  // spins s0, s0+1 (s0 even) of every colour: one half of each int4
+  __device__ __forceinline__ void load_pair_raw(int i, int s0, cx<float> h[2][3], float& sc) const {
+    sc = __ldg(norm + i) * (1.0f / 32767.0f);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
       const int2* p = reinterpret_cast<const int2*>(v + c * stride + i);
-      int2 t = __ldg(p + (s0 >> 1));
-      const short* q = reinterpret_cast<const short*>(&t);
-      h[0][c] = mkc(q2f(q[0], scale), q2f(q[1], scale));
-      h[1][c] = mkc(q2f(q[2], scale), q2f(q[3], scale));
+      const int2 t = __ldg(p + (s0 >> 1));
+      const float2 a = s16x2_to_f2(t.x), b = s16x2_to_f2(t.y);
+      h[0][c] = mkc(a.x, a.y);
+      h[1][c] = mkc(b.x, b.y);
     }
   }
   __device__ __forceinline__ void store(int i, const Spinor<float>& s) const {
@@ -267,17 +316,16 @@ struct SpinorView<Prec::F16> {
     for (int a = 0; a < 4; a++)
 #pragma unroll
       for (int b = 0; b < 3; b++) m = fmaxf(m, fmaxf(fabsf(s.c[a][b].x), fabsf(s.c[a][b].y)));
-    float inv = m > 0.f ? 32767.0f / m : 0.f;
+    const float inv = m > 0.f ? 32767.0f / m : 0.f;
     norm[i] = m;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      short q[8];
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        q[2 * j] = f2q(s.c[j][k].x, inv);
-        q[2 * j + 1] = f2q(s.c[j][k].y, inv);
-      }
-      v[k * stride + i] = *reinterpret_cast<int4*>(q);
+      int4 t;
+      t.x = (int)f2_to_s16x2(s.c[0][k].x, s.c[0][k].y, inv);
+      t.y = (int)f2_to_s16x2(s.c[1][k].x, s.c[1][k].y, inv);
+      t.z = (int)f2_to_s16x2(s.c[2][k].x, s.c[2][k].y, inv);
+      t.w = (int)f2_to_s16x2(s.c[3][k].x, s.c[3][k].y, inv);
+      v[k * stride + i] = t;
     }
   }
 };
@@ -348,15 +396,17 @@ struct GaugeView<Prec::F16> {
   short4* v;  // [4][2][3][stride], entries scaled by 32767
   int stride;
   __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
-    const short4* b = v + (size_t)((mu * 2 + eo) * 3) * stride + i;
+    // one short4 = two complex entries = two 32-bit words
+    const uint2* b = reinterpret_cast<const uint2*>(v) + (size_t)((mu * 2 + eo) * 3) * stride + i;
     const float sc = 1.0f / 32767.0f;
-    short4 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
-    u.m[0][0] = mkc(t0.x * sc, t0.y * sc);
-    u.m[1][0] = mkc(t0.z * sc, t0.w * sc);
-    u.m[2][0] = mkc(t1.x * sc, t1.y * sc);
-    u.m[0][1] = mkc(t1.z * sc, t1.w * sc);
-    u.m[1][1] = mkc(t2.x * sc, t2.y * sc);
-    u.m[2][1] = mkc(t2.z * sc, t2.w * sc);
+    const uint2 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
+    float2 e;
+    e = s16x2_to_f2(t0.x); u.m[0][0] = mkc(e.x * sc, e.y * sc);
+    e = s16x2_to_f2(t0.y); u.m[1][0] = mkc(e.x * sc, e.y * sc);
+    e = s16x2_to_f2(t1.x); u.m[2][0] = mkc(e.x * sc, e.y * sc);
+    e = s16x2_to_f2(t1.y); u.m[0][1] = mkc(e.x * sc, e.y * sc);
+    e = s16x2_to_f2(t2.x); u.m[1][1] = mkc(e.x * sc, e.y * sc);
+    e = s16x2_to_f2(t2.y); u.m[2][1] = mkc(e.x * sc, e.y * sc);
     reconstruct_col3(u);
   }
 };
@@ -380,6 +430,10 @@ struct CloverView<Prec::F64> {
       a[k] = mkc(t.x, t.y);
     }
   }
+  __device__ __forceinline__ void load_block_raw(int i, int chi, cx<double> a[18], double& sc) const {
+    load_block(i, chi, a);
+    sc = 1.0;
+  }
 };
 
 template <>
@@ -395,6 +449,10 @@ struct CloverView<Prec::F32> {
       a[2 * k + 1] = mkc(t.z, t.w);
     }
   }
+  __device__ __forceinline__ void load_block_raw(int i, int chi, cx<float> a[18], float& sc) const {
+    load_block(i, chi, a);
+    sc = 1.0f;
+  }
 };
 
 template <>
@@ -403,18 +461,29 @@ struct CloverView<Prec::F16> {
   int4* v;  // [9][stride], 8 int16 = 4 slots each
   float* norm;
   int stride;
+  // slots chi*18 .. chi*18+17 live in int4 numbers (chi*18)/4 .. (chi*18+17)/4:
+  // block 0 in words 0-4, block 1 in words 4-8
   __device__ __forceinline__ void load_block(int i, int chi, cx<float> a[18]) const {
-    float scale = __ldg(norm + i) * (1.0f / 32767.0f);
-    // slots chi*18 .. chi*18+17 live in int4 numbers (chi*18)/4 .. (chi*18+17)/4
+    float sc;
+    load_block_raw(i, chi, a, sc);
+#pragma unroll
+    for (int k = 0; k < 18; k++) a[k] = sc * a[k];
+  }
+  // raw int16 values; the block is raw * sc (applied to the block's output)
+  __device__ __forceinline__ void load_block_raw(int i, int chi, cx<float> a[18], float& sc) const {
+    sc = __ldg(norm + i) * (1.0f / 32767.0f);
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-      int word = chi * 4 + k;  // block 0: words 0-4, block 1: words 4-8
-      int4 t = __ldg(v + word * stride + i);
-      const short* q = reinterpret_cast<const short*>(&t);
+      const int word = chi * 4 + k;
+      const int4 t = __ldg(v + word * stride + i);
+      const unsigned w[4] = {(unsigned)t.x, (unsigned)t.y, (unsigned)t.z, (unsigned)t.w};
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        int slot = 4 * word + j - chi * 18;
-        if (slot >= 0 && slot < 18) a[slot] = mkc(q[2 * j] * scale, q[2 * j + 1] * scale);
+        const int slot = 4 * word + j - chi * 18;
+        if (slot >= 0 && slot < 18) {
+          const float2 e = s16x2_to_f2(w[j]);
+          a[slot] = mkc(e.x, e.y);
+        }
       }
     }
   }
@@ -456,21 +525,24 @@ __device__ __forceinline__ void clover_block_mv(const cx<R>* a, const cx<R> x[6]
 template <Prec P, typename R>
 __device__ __forceinline__ void clover_apply(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out) {
   cx<R> x[6], y[6], a[18];
+  R sc;
 #pragma unroll
   for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3];
-  A.load_block(i, 0, a);
+  A.load_block_raw(i, 0, a, sc);
   clover_block_mv(a, x, y);
 #pragma unroll
   for (int k = 0; k < 6; k++) {
+    y[k] = sc * y[k];
     out.c[k / 3][k % 3] = y[k];
     out.c[k / 3 + 2][k % 3] = y[k];
   }
 #pragma unroll
   for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] - in.c[k / 3 + 2][k % 3];
-  A.load_block(i, 1, a);
+  A.load_block_raw(i, 1, a, sc);
   clover_block_mv(a, x, y);
 #pragma unroll
   for (int k = 0; k < 6; k++) {
+    y[k] = sc * y[k];
     out.c[k / 3][k % 3] = out.c[k / 3][k % 3] + y[k];
     out.c[k / 3 + 2][k % 3] = out.c[k / 3 + 2][k % 3] - y[k];
   }
@@ -601,37 +673,40 @@ __device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Si
   zero(b);
 #pragma unroll
   for (int mu = 3; mu >= 0; mu--) {
-    // forward hop
+    // forward hop; the spinor's storage scale (int16 fields) is applied once
+    // to the transported half spinor, together with the boundary sign
     {
       int j = neighbour(g, st, i, mu, true);
       cx<R> h[2][3], f[2][3];
+      R sc;
       if (mu == 3) {
         // (1 -+ gamma_4) keeps two spins: (3,4) for d, (1,2) for d_dag
-        in.load_pair(j, DAG ? 0 : 2, h);
+        in.load_pair_raw(j, DAG ? 0 : 2, h, sc);
       } else {
         Spinor<R> p;
-        in.load(j, p);
+        in.load_raw(j, p, sc);
         project<R, DAG>(p, mu, true, h);
       }
       Link<R> u;
       U.load(mu, e, i, u);
-      mul_u(u, h, (R)hop_sign(g, st, mu, true), f);
+      mul_u(u, h, (R)hop_sign(g, st, mu, true) * sc, f);
       recon_fwd<R, DAG>(b, mu, f);
     }
     // backward hop
     {
       int j = neighbour(g, st, i, mu, false);
       cx<R> h[2][3], f[2][3];
+      R sc;
       if (mu == 3) {
-        in.load_pair(j, DAG ? 2 : 0, h);
+        in.load_pair_raw(j, DAG ? 2 : 0, h, sc);
       } else {
         Spinor<R> p;
-        in.load(j, p);
+        in.load_raw(j, p, sc);
         project<R, DAG>(p, mu, false, h);
       }
       Link<R> u;
       U.load(mu, o, j, u);
-      mul_ud(u, h, (R)hop_sign(g, st, mu, false), f);
+      mul_ud(u, h, (R)hop_sign(g, st, mu, false) * sc, f);
       recon_bwd<R, DAG>(b, mu, f);
     }
   }

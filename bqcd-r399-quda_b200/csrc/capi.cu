@@ -298,6 +298,9 @@ struct KernelTimer {
 };
 
 constexpr int kStalled = 100;  // internal: the sloppy precision stopped converging
+// a reliable update at least every kRuEvery sloppy iterations, so that a
+// stagnating true residual is seen even when the iterated one keeps falling
+constexpr int kRuEvery = 1000;
 
 // Core CG on device-resident x, b (F64, device layout).  Solves (W^+W) x = b.
 //   sloppy == F64: plain FP64 CG (cg.F90)
@@ -358,6 +361,8 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   h.maxiter = maxiter;
   h.delta2 = sloppy == Prec::F64 ? 0.0 : delta * delta;
   h.maxr2 = rtr;
+  h.ru_every = sloppy == Prec::F64 ? 0 : kRuEvery;
+  h.last_ru = 0;
   double best = rtr;  // smallest true |r|^2 so far
   int stall = 0;      // reliable updates in a row without progress
   bool stalled = false;
@@ -425,6 +430,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     h.beta = rtrue / h.rtr_old;
     h.rtr = rtrue;
     h.maxr2 = rtrue;
+    h.last_ru = h.iter;
     h.done = 0;
     { int st_ = write_cg(c); if (st_) return st_; }
     launch_p_reorth(g, sloppy, p, rs, rpc, h.beta, c->stream);
@@ -567,6 +573,8 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
     h.maxiter = maxiter;
     h.delta2 = delta * delta;
     h.maxr2 = r2;
+    h.ru_every = kRuEvery;
+    h.last_ru = 0;
     best[k] = r2;
     info[k].b2 = b2;
     if (!(r2 == r2)) { h.done = 4; fin[k] = 1; }
@@ -623,6 +631,7 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
       h.beta = rt / h.rtr_old;
       h.rtr = rt;
       h.maxr2 = rt;
+      h.last_ru = h.iter;
       h.done = 0;
       resume.push_back(k);
     }

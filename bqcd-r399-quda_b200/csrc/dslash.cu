@@ -14,12 +14,18 @@ namespace bqcdg {
 // Resident CTAs per SM requested from the register allocator.  The reduced-
 // precision stencils move few bytes per thread, so latency hiding needs more
 // warps in flight than the FP64 ones (whose per-thread loads are 2-4x larger).
+// The second pass carries the clover block, the input spinor and (fused into
+// CG) x, r and p besides the hop, so it gets a larger register budget.
 #ifndef BQCDG_SLOPPY_MIN_BLOCKS
-#define BQCDG_SLOPPY_MIN_BLOCKS 8
+#define BQCDG_SLOPPY_MIN_BLOCKS 6
+#endif
+#ifndef BQCDG_SLOPPY_MIN_BLOCKS2
+#define BQCDG_SLOPPY_MIN_BLOCKS2 5
 #endif
 template <Prec P>
 struct Occ {
   static constexpr int min_blocks = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS;
+  static constexpr int min_blocks2 = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS2;
 };
 
 template <Prec P>
@@ -271,7 +277,7 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
 }
 
 template <Prec P, bool DAG, bool REDUCE>
-__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
+__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
                                                   const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                                                   double hval, double rho, RedScratch red, double* norm_out,
                                                   CgScalars* cg, int nr) {
@@ -349,7 +355,7 @@ struct XR<Prec::F32> {
 };
 
 template <Prec P, Prec XP>
-__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
+__global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
                                                      RedScratch red, CgScalars* cgs, int nr) {
@@ -404,6 +410,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_cg_pass4(Geom g,
       else if (rtr <= cg->stop_rtr) cg->done = 1;
       else if (cg->iter >= cg->maxiter) cg->done = 3;
       else if (rtr < cg->delta2 * cg->maxr2) cg->done = 2;  // reliable update (|r| < delta max|r|)
+      else if (cg->ru_every > 0 && cg->iter - cg->last_ru >= cg->ru_every) cg->done = 2;  // periodic check
       red.counter[tl.rhs] = 0;
     }
   }

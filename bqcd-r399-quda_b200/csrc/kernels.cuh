@@ -50,6 +50,8 @@ struct CgScalars {
   int pad;
   double delta2;    // sloppy solver: reliable update when rtr < delta2 * maxr2 (0: never)
   double maxr2;     // largest |r|^2 since the last reliable update
+  int last_ru;      // iteration of the last reliable update
+  int ru_every;     // also update after this many iterations without one (0: never)
 };
 
 struct OpParams {

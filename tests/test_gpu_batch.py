@@ -53,5 +53,5 @@ def test_batch_retires_converged_rhs(setup, bq):
     lat.field_gauss(h1, 0.5)
     hx = [lat.field(zero), lat.field(zero)]
     infos = lat.solve_batch(hx, [h0, h1], para, tol=1e-10, relative=False, block=2)
-    assert infos[0].niter == 0 and infos[0].converged == 1
-    assert infos[1].converged == 1 and infos[1].niter > 0
+    assert infos[0].niter == 0 and infos[0].converged == 1, infos[0].as_dict()
+    assert infos[1].converged == 1 and infos[1].niter > 0, infos[1].as_dict()

@@ -5,7 +5,8 @@ flipped links; the clover blocks are rebuilt on the device from each perturbed
 gauge field).  dsf (dsf.F90:28) adds p -= step * dS/domega_j for
 U -> exp(i omega_j lambda_j) U (hmc_u.F90:53-60), so along a direction h
 (h_j per link) the derivative is  dS/deps = -(p_new - p_old).h / step.
-Checked along 16 random su(3) directions with eps = 1e-5 to 1e-7 relative.
+Checked along 16 random su(3) directions by a fourth-order difference
+quotient at eps = 1e-4, to 1e-7 relative.
 """
 import numpy as np
 import pytest
@@ -41,13 +42,16 @@ def perturb(oracle, u, h, eps):
 
 
 def action(lat, g, oracle, u, phi, para, csw_kappa):
+    """S = phi^+ A^-1 phi (A = W^+W) from the Galerkin estimate
+    2 Re <phi,x> - <x,Ax>, whose error is quadratic in the solver's: the
+    fourth-order difference quotient at eps = 1e-4 needs S to ~1e-15 relative."""
     uf = g.flip_bc(u.copy())
     lat.load_gauge(uf, flipped=True)
     lat.clover_init(csw_kappa)
     x, info = lat.solve(np.zeros_like(phi), phi, para, precision=0, tol=1e-13, rho=para.rho)
     assert info.converged
-    wx = lat.w_mult(x, para)
-    return float(np.vdot(wx, wx).real)
+    ax = lat.w_dagger_w(x, para)
+    return float(2.0 * np.vdot(phi, x).real - np.vdot(x, ax).real)
 
 
 @pytest.mark.parametrize("csw", [0.0, 1.9192])
@@ -71,13 +75,16 @@ def test_dsf_matches_finite_differences(oracle, bq, csw):
         step = 1.0
         p0 = np.zeros((4, 2, lat.volh, 8))
         dS = -lat.dsf(p0.copy(), step, para, a, b) / step          # dS/domega_j per link
-        eps = 1e-5
+        # fourth-order central difference: truncation O(eps^4) is negligible,
+        # and eps = 1e-4 keeps the rounding noise of S (~1e-12 absolute)
+        # divided by eps well under the tolerance
+        eps = 1e-4
         errs = []
         for _ in range(16):
             h = rng.standard_normal((4, 2, lat.volh, 8))
-            sp = action(lat, g, oracle, perturb(oracle, u, h, eps), phi, para, csw * kappa)
-            sm = action(lat, g, oracle, perturb(oracle, u, h, -eps), phi, para, csw * kappa)
-            fd = (sp - sm) / (2 * eps)
+            s = {k: action(lat, g, oracle, perturb(oracle, u, h, k * eps), phi, para, csw * kappa)
+                 for k in (-2, -1, 1, 2)}
+            fd = (8.0 * (s[1] - s[-1]) - (s[2] - s[-2])) / (12.0 * eps)
             an = float(np.sum(dS * h))
             errs.append(abs(fd - an) / abs(an))
         assert max(errs) < 1e-7, errs
