@@ -209,6 +209,38 @@ int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, in
  * Ainv_oo) at the given precision, n launches */
 int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precision, int n, double *ms);
 
+/* ---- allocation-free operator ------------------------------------------- */
+/* This entry point has no counterpart in the reference.  It is for callers
+ * that cannot let the library allocate device memory: a framework whose pool
+ * or arena allocator owns every buffer, or code that must not call cudaMalloc
+ * (which may synchronise the device) in a latency-critical region.  It needs
+ * no context.
+ *
+ * out = (W^+W) in with W = M~ + p->rho (p->rho = 0: mtdagmt), in FP64.  All
+ * arrays are caller-owned DEVICE memory in the library's device layout, with
+ * stride = volh rounded up to a multiple of 64:
+ *   gauge     double2[4][2][9][stride]  periodic links, u(row,col) at k = col*3+row
+ *   a_even    double2[36][stride]       conf%a of the even sites (chi*18 + slot)
+ *   ainv_odd  double2[36][stride]       conf%i of the odd sites (may be NULL for csw = 0)
+ *   in, out   double2[12][stride]       even-site spinors, k = colour*4+spin
+ * The fermion boundary signs bc are applied inside the kernels.  stream is a
+ * cudaStream_t (NULL: the default stream); the call only enqueues work.
+ *
+ * Its two intermediate fields live in one static device array sized for
+ * volh <= BQCDG_NOALLOC_MAX_VOLH (6.3 MB, held by every GPU that loads the
+ * library until the process exits); larger lattices are rejected with
+ * BQCDG_EINVAL.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture, and from one host thread at a time (the
+ * look-up is not locked).  All calls on a device share the array and
+ * it keeps the last call's contents: calls that overlap on the GPU race.
+ * Nothing in it needs to start at zero, since each call writes every site it
+ * later reads. */
+#define BQCDG_NOALLOC_MAX_VOLH 16384
+int bqcdg_mdagm_noalloc(const int L[4], const int bc[4], const double *gauge, const double *a_even,
+                        const double *ainv_odd, const bqcdg_params *p, const double *in, double *out,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif

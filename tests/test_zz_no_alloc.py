@@ -1,0 +1,100 @@
+"""The allocation-free operator entry point bqcdg_mdagm_noalloc, called through
+the C ABI on device buffers that the caller (this test, through torch) owns.
+
+It serves callers that cannot let the library allocate: everything it needs
+besides the caller's inputs and outputs sits in a fixed static device array.
+Its result must equal the context-based entry points (bqcdg_mtdagmt /
+bqcdg_w_dagger_w on host arrays) to the FP64 operator tolerance, on two calls
+in a row (the second reuses the static scratch left by the first), and a
+lattice larger than the stated maximum must be rejected.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-13
+
+
+def stride_of(volh):
+    return (volh + 63) // 64 * 64
+
+
+def dev(arr, torch):
+    return torch.from_numpy(np.ascontiguousarray(arr)).to("cuda")
+
+
+def gauge_layout(u, volh):
+    """GAUGE_FIELD (4,2,volh,3,3)[col][row] -> double2[4][2][9][stride]."""
+    s = stride_of(volh)
+    out = np.zeros((4, 2, 9, s), np.complex128)
+    out[:, :, :, :volh] = u.reshape(4, 2, volh, 9).transpose(0, 1, 3, 2)
+    return out
+
+
+def clover_layout(c_eo, volh):
+    """one parity of CLOVER_FIELD_A (volh,2,18) -> double2[36][stride]."""
+    out = np.zeros((36, stride_of(volh)), np.complex128)
+    out[:, :volh] = c_eo.reshape(volh, 36).T
+    return out
+
+
+def spinor_layout(x, volh):
+    out = np.zeros((12, stride_of(volh)), np.complex128)
+    out[:, :volh] = x.reshape(volh, 12).T
+    return out
+
+
+def spinor_from_layout(y, volh):
+    return np.ascontiguousarray(y[:, :volh].T).reshape(volh, 3, 4)
+
+
+@pytest.fixture(scope="module")
+def fn(bq):
+    f = bq.lib().bqcdg_mdagm_noalloc
+    f.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                  C.POINTER(bq.Params), C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    return f
+
+
+@pytest.mark.parametrize("rho", [0.0, 0.1])
+def test_noalloc_matches_context_entry_point_twice(oracle, bq, fn, rho):
+    import torch
+    L, bc = (8, 8, 8, 8), (1, 1, 1, -1)
+    g = oracle.Geom(L, bc)
+    oracle.ranset(31)
+    u = g.hot()
+    kappa, csw = 0.13, 1.9192
+    a, ai, b = g.clover_init(u, csw * kappa)
+    para = bq.HmcPara(kappa=kappa, csw=csw, rho=rho)
+    volh = g.volh
+    d_u = dev(gauge_layout(u, volh), torch)
+    d_a = dev(clover_layout(a[0], volh), torch)
+    d_ai = dev(clover_layout(ai[1], volh), torch)
+    d_in = torch.zeros((12, stride_of(volh)), dtype=torch.complex128, device="cuda")
+    d_out = torch.zeros_like(d_in)
+    Li, bci = (C.c_int * 4)(*L), (C.c_int * 4)(*bc)
+    prm = para.params()
+    with bq.Lattice(L, bc) as lat:
+        lat.load_gauge(u, flipped=False)
+        lat.load_clover(a, ai, b)
+        for call in range(2):
+            psi = g.gauss_spinor(0)
+            d_in.copy_(dev(spinor_layout(psi, volh), torch))
+            st = fn(Li, bci, d_u.data_ptr(), d_a.data_ptr(), d_ai.data_ptr(), C.byref(prm), d_in.data_ptr(),
+                    d_out.data_ptr(), None)
+            assert st == bq.OK
+            torch.cuda.synchronize()
+            got = spinor_from_layout(d_out.cpu().numpy(), volh)
+            ref = lat.w_dagger_w(psi, para) if rho else lat.mtdagmt(psi, para)
+            assert np.linalg.norm(got - ref) <= TOL64 * np.linalg.norm(ref), call
+
+
+def test_noalloc_rejects_lattices_beyond_the_static_scratch(bq, fn):
+    L = (16, 16, 16, 16)           # volh 32768 > BQCDG_NOALLOC_MAX_VOLH
+    prm = bq.Params(0.13, 0.0, 0.0, 0.0)
+    one = C.c_void_p(1)            # never dereferenced: the size check comes first
+    st = fn((C.c_int * 4)(*L), (C.c_int * 4)(1, 1, 1, -1), one, one, one, C.byref(prm), one, one, None)
+    assert st == bq.EINVAL
