@@ -105,6 +105,23 @@ __device__ __forceinline__ void zero(Spinor<R>& s) {
 // ---------------------------------------------------------------------------
 // geometry: even/odd index i = ilex/2 (index.F90:58-76), parity (x+y+z+t)%2
 // ---------------------------------------------------------------------------
+// n / d for 0 <= n < 2^31 as (umulhi(n, m) + n) >> l, with l = ceil(log2 d)
+// and m = floor(2^32 (2^l - d) / d) + 1 (the round-up method of Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994)
+struct FastDiv {
+  unsigned d, m;
+  int l;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  int l = 0;
+  while ((1ull << l) < d) l++;
+  const unsigned long long m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
+  return FastDiv{d, (unsigned)m, l};
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
+  return (__umulhi(n, f.m) + n) >> f.l;
+}
+
 struct Geom {
   int L[4];
   int Lxh;
@@ -112,7 +129,14 @@ struct Geom {
   int stride;      // padded per-component stride of every field
   int bcsign[4];   // fermion boundary sign per direction (+1 / -1)
   int rec12;       // FP64 stencil links stored as 12 reals (columns 1,2)
+  FastDiv dxh, d1, d2;  // division by Lxh, L[1], L[2] (geom_finish)
 };
+// fills the derived members once L and Lxh are set
+inline void geom_finish(Geom& g) {
+  g.dxh = make_fastdiv((unsigned)g.Lxh);
+  g.d1 = make_fastdiv((unsigned)g.L[1]);
+  g.d2 = make_fastdiv((unsigned)g.L[2]);
+}
 
 struct Site {
   int x[4];
@@ -121,12 +145,12 @@ struct Site {
 
 __device__ __forceinline__ Site site_coords(const Geom& g, int i, int parity) {
   Site s;
-  int xh = i % g.Lxh;
-  int r = i / g.Lxh;
-  s.x[1] = r % g.L[1];
-  r /= g.L[1];
-  s.x[2] = r % g.L[2];
-  s.x[3] = r / g.L[2];
+  const int r = (int)fdiv((unsigned)i, g.dxh);
+  const int xh = i - r * g.Lxh;
+  const int r2 = (int)fdiv((unsigned)r, g.d1);
+  s.x[1] = r - r2 * g.L[1];
+  s.x[3] = (int)fdiv((unsigned)r2, g.d2);
+  s.x[2] = r2 - s.x[3] * g.L[2];
   s.x[0] = 2 * xh + ((s.x[1] + s.x[2] + s.x[3] + parity) & 1);
   s.base = i - xh;
   return s;
@@ -199,6 +223,13 @@ struct SpinorView<Prec::F64> {
     load_pair(i, s0, h);
     sc = 1.0;
   }
+  __device__ __forceinline__ void store_scaled(int i, Spinor<double> s, double extra) const {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) s.c[a][b] = extra * s.c[a][b];
+    store(i, s);
+  }
 };
 
 template <>
@@ -240,23 +271,35 @@ struct SpinorView<Prec::F32> {
     load_pair(i, s0, h);
     sc = 1.0f;
   }
+  __device__ __forceinline__ void store_scaled(int i, Spinor<float> s, float extra) const {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) s.c[a][b] = extra * s.c[a][b];
+    store(i, s);
+  }
 };
 
 
-// int16 <-> float without the quarter-rate I2F/F2I conversions.  Load: bias
-// the pair to unsigned (q + 32768), splice each half into the mantissa of
-// 2^23 with a byte permute and subtract 2^23 + 2^15 -- exact for every int16.
-__device__ __forceinline__ float2 s16x2_to_f2(unsigned w) {
-  const unsigned u = w ^ 0x80008000u;
-  const float lo = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7610)) - 8421376.0f;
-  const float hi = __uint_as_float(__byte_perm(u, 0x4B000000u, 0x7632)) - 8421376.0f;
-  return make_float2(lo, hi);
+// int16 fields are stored offset-binary: u = q + 32768 for q in [-32767, 32767].
+// Conversions avoid the quarter-rate I2F/F2I instructions.  Load: splice u into
+// the mantissa of 2^23 with a byte permute, giving the float 2^23 + u exactly
+// ("biased" value q + kQBias); subtracting kQBias leaves q.  Store:
+// a + kQStore rounds a (|a| <= 32767.5) to the nearest integer and leaves
+// q + 32768 in the low 16 bits of the mantissa.
+constexpr float kQBias = 8421376.0f;    // 2^23 + 2^15
+constexpr float kQStore = 12615680.0f;  // 1.5 * 2^23 + 2^15
+__device__ __forceinline__ float2 u16x2_biased(unsigned w) {
+  return make_float2(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)),
+                     __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
 }
-// Store: a + 1.5*2^23 rounds a (|a| <= 32767) to the nearest integer and
-// leaves it, in two's complement, in the low 16 bits of the mantissa.
-__device__ __forceinline__ unsigned f2_to_s16x2(float a, float b, float scale) {
-  const unsigned ia = __float_as_uint(fmaf(a, scale, 12582912.0f));
-  const unsigned ib = __float_as_uint(fmaf(b, scale, 12582912.0f));
+__device__ __forceinline__ float2 u16x2_to_f2(unsigned w) {
+  const float2 b = u16x2_biased(w);
+  return make_float2(b.x - kQBias, b.y - kQBias);
+}
+__device__ __forceinline__ unsigned f2_to_u16x2(float a, float b, float scale) {
+  const unsigned ia = __float_as_uint(fmaf(a, scale, kQStore));
+  const unsigned ib = __float_as_uint(fmaf(b, scale, kQStore));
   return __byte_perm(ia, ib, 0x5410);
 }
 
@@ -291,7 +334,7 @@ struct SpinorView<Prec::F16> {
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const int4 t = __ldg(v + k * stride + i);
-      const float2 a = s16x2_to_f2(t.x), b = s16x2_to_f2(t.y), c = s16x2_to_f2(t.z), d = s16x2_to_f2(t.w);
+      const float2 a = u16x2_to_f2(t.x), b = u16x2_to_f2(t.y), c = u16x2_to_f2(t.z), d = u16x2_to_f2(t.w);
       s.c[0][k] = mkc(a.x, a.y);
       s.c[1][k] = mkc(b.x, b.y);
       s.c[2][k] = mkc(c.x, c.y);
@@ -305,29 +348,46 @@ struct SpinorView<Prec::F16> {
     for (int c = 0; c < 3; c++) {
       const int2* p = reinterpret_cast<const int2*>(v + c * stride + i);
       const int2 t = __ldg(p + (s0 >> 1));
-      const float2 a = s16x2_to_f2(t.x), b = s16x2_to_f2(t.y);
+      const float2 a = u16x2_to_f2(t.x), b = u16x2_to_f2(t.y);
       h[0][c] = mkc(a.x, a.y);
       h[1][c] = mkc(b.x, b.y);
     }
   }
-  __device__ __forceinline__ void store(int i, const Spinor<float>& s) const {
+  // biased values (q + kQBias, see u16x2_biased) of all 12 components,
+  // F[spin][colour] = (re, im); the true value is (F - kQBias) * sc
+  __device__ __forceinline__ void load_biased(int i, float2 F[4][3], float& sc) const {
+    sc = __ldg(norm + i) * (1.0f / 32767.0f);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int4 t = __ldg(v + k * stride + i);
+      F[0][k] = u16x2_biased(t.x);
+      F[1][k] = u16x2_biased(t.y);
+      F[2][k] = u16x2_biased(t.z);
+      F[3][k] = u16x2_biased(t.w);
+    }
+  }
+  // stores s * extra: a common factor of the site (extra > 0) goes into the
+  // norm instead of being multiplied into the 24 components
+  __device__ __forceinline__ void store_scaled(int i, const Spinor<float>& s, float extra) const {
     float m = 0.f;
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
       for (int b = 0; b < 3; b++) m = fmaxf(m, fmaxf(fabsf(s.c[a][b].x), fabsf(s.c[a][b].y)));
-    const float inv = m > 0.f ? 32767.0f / m : 0.f;
-    norm[i] = m;
+    // below 1e-30 the quotient could overflow: such a site is stored as zero
+    const float inv = m > 1e-30f ? __fdividef(32767.0f, m) : 0.f;
+    norm[i] = m * extra;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       int4 t;
-      t.x = (int)f2_to_s16x2(s.c[0][k].x, s.c[0][k].y, inv);
-      t.y = (int)f2_to_s16x2(s.c[1][k].x, s.c[1][k].y, inv);
-      t.z = (int)f2_to_s16x2(s.c[2][k].x, s.c[2][k].y, inv);
-      t.w = (int)f2_to_s16x2(s.c[3][k].x, s.c[3][k].y, inv);
+      t.x = (int)f2_to_u16x2(s.c[0][k].x, s.c[0][k].y, inv);
+      t.y = (int)f2_to_u16x2(s.c[1][k].x, s.c[1][k].y, inv);
+      t.z = (int)f2_to_u16x2(s.c[2][k].x, s.c[2][k].y, inv);
+      t.w = (int)f2_to_u16x2(s.c[3][k].x, s.c[3][k].y, inv);
       v[k * stride + i] = t;
     }
   }
+  __device__ __forceinline__ void store(int i, const Spinor<float>& s) const { store_scaled(i, s, 1.0f); }
 };
 
 // links --------------------------------------------------------------------
@@ -370,6 +430,10 @@ struct GaugeView<Prec::F64> {
         u.m[r][c] = mkc(t.x, t.y);
       }
   }
+  __device__ __forceinline__ void load_raw(int mu, int eo, int i, Link<double>& u, double& lsc) const {
+    load(mu, eo, i, u);
+    lsc = 1.0;
+  }
 };
 
 template <>
@@ -388,26 +452,43 @@ struct GaugeView<Prec::F32> {
     u.m[2][1] = mkc(t2.z, t2.w);
     reconstruct_col3(u);
   }
+  __device__ __forceinline__ void load_raw(int mu, int eo, int i, Link<float>& u, float& lsc) const {
+    load(mu, eo, i, u);
+    lsc = 1.0f;
+  }
 };
 
 template <>
 struct GaugeView<Prec::F16> {
   using R = float;
-  short4* v;  // [4][2][3][stride], entries scaled by 32767
+  short4* v;  // [4][2][3][stride], offset-binary entries of 32767 u
   int stride;
-  __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
+  // the link times 32767 (U = u * lsc): columns 1, 2 as stored, the third
+  // rebuilt from them and brought to the same scale, so that one factor per
+  // hop replaces a multiply of every entry
+  __device__ __forceinline__ void load_raw(int mu, int eo, int i, Link<float>& u, float& lsc) const {
     // one short4 = two complex entries = two 32-bit words
     const uint2* b = reinterpret_cast<const uint2*>(v) + (size_t)((mu * 2 + eo) * 3) * stride + i;
-    const float sc = 1.0f / 32767.0f;
     const uint2 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
     float2 e;
-    e = s16x2_to_f2(t0.x); u.m[0][0] = mkc(e.x * sc, e.y * sc);
-    e = s16x2_to_f2(t0.y); u.m[1][0] = mkc(e.x * sc, e.y * sc);
-    e = s16x2_to_f2(t1.x); u.m[2][0] = mkc(e.x * sc, e.y * sc);
-    e = s16x2_to_f2(t1.y); u.m[0][1] = mkc(e.x * sc, e.y * sc);
-    e = s16x2_to_f2(t2.x); u.m[1][1] = mkc(e.x * sc, e.y * sc);
-    e = s16x2_to_f2(t2.y); u.m[2][1] = mkc(e.x * sc, e.y * sc);
-    reconstruct_col3(u);
+    e = u16x2_to_f2(t0.x); u.m[0][0] = mkc(e.x, e.y);
+    e = u16x2_to_f2(t0.y); u.m[1][0] = mkc(e.x, e.y);
+    e = u16x2_to_f2(t1.x); u.m[2][0] = mkc(e.x, e.y);
+    e = u16x2_to_f2(t1.y); u.m[0][1] = mkc(e.x, e.y);
+    e = u16x2_to_f2(t2.x); u.m[1][1] = mkc(e.x, e.y);
+    e = u16x2_to_f2(t2.y); u.m[2][1] = mkc(e.x, e.y);
+    reconstruct_col3(u);  // 32767^2 times the true column
+    lsc = 1.0f / 32767.0f;
+#pragma unroll
+    for (int r = 0; r < 3; r++) u.m[r][2] = lsc * u.m[r][2];
+  }
+  __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
+    float lsc;
+    load_raw(mu, eo, i, u, lsc);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) u.m[r][c] = lsc * u.m[r][c];
   }
 };
 
@@ -481,7 +562,7 @@ struct CloverView<Prec::F16> {
       for (int j = 0; j < 4; j++) {
         const int slot = 4 * word + j - chi * 18;
         if (slot >= 0 && slot < 18) {
-          const float2 e = s16x2_to_f2(w[j]);
+          const float2 e = u16x2_to_f2(w[j]);
           a[slot] = mkc(e.x, e.y);
         }
       }
@@ -521,31 +602,40 @@ __device__ __forceinline__ void clover_block_mv(const cx<R>* a, const cx<R> x[6]
 }
 
 // out = A in on one site, both chiral blocks (clover_mult_a.F90:45-95): the
-// blocks act on x+- = psi(spin 1,2) +- psi(spin 3,4).
+// blocks act on x+- = psi(spin 1,2) +- psi(spin 3,4).  The _raw form leaves
+// out = (A / sc) in, sc the storage scale of the site's blocks (1 except for
+// int16), for callers that fold sc into a later factor.
 template <Prec P, typename R>
-__device__ __forceinline__ void clover_apply(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out) {
+__device__ __forceinline__ void clover_apply_raw(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out,
+                                                 R& sc) {
   cx<R> x[6], y[6], a[18];
-  R sc;
 #pragma unroll
   for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3];
   A.load_block_raw(i, 0, a, sc);
   clover_block_mv(a, x, y);
 #pragma unroll
   for (int k = 0; k < 6; k++) {
-    y[k] = sc * y[k];
     out.c[k / 3][k % 3] = y[k];
     out.c[k / 3 + 2][k % 3] = y[k];
   }
 #pragma unroll
   for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] - in.c[k / 3 + 2][k % 3];
-  A.load_block_raw(i, 1, a, sc);
+  A.load_block_raw(i, 1, a, sc);  // both blocks of a site share one scale
   clover_block_mv(a, x, y);
 #pragma unroll
   for (int k = 0; k < 6; k++) {
-    y[k] = sc * y[k];
     out.c[k / 3][k % 3] = out.c[k / 3][k % 3] + y[k];
     out.c[k / 3 + 2][k % 3] = out.c[k / 3 + 2][k % 3] - y[k];
   }
+}
+template <Prec P, typename R>
+__device__ __forceinline__ void clover_apply(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out) {
+  R sc;
+  clover_apply_raw(A, i, in, out, sc);
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) out.c[a][b] = sc * out.c[a][b];
 }
 
 // ---------------------------------------------------------------------------
@@ -569,6 +659,37 @@ __device__ __forceinline__ void project(const Spinor<R>& p, int mu, bool fwd, cx
     } else {
       h[0][c] = p.c[0][c] + sg * itimes(p.c[2][c]);
       h[1][c] = p.c[1][c] - sg * itimes(p.c[3][c]);
+    }
+  }
+}
+
+// sa*(A - kQBias) + sb*(B - kQBias) for biased int16 values A, B; the signs
+// are constants once the hop loop is unrolled.  A difference of biased values
+// is exact in one add, a sum takes two (every intermediate is an integer
+// below 2^24).
+__device__ __forceinline__ float comb_biased(float A, float B, float sa, float sb) {
+  if (sa == -sb) return sa > 0.f ? A - B : B - A;
+  const float t = (A - 2.0f * kQBias) + B;
+  return sa > 0.f ? t : -t;
+}
+// project() on biased int16 components (SpinorView<F16>::load_biased): the
+// same half spinor, up to the site's storage scale, without first removing
+// the bias from every component
+template <bool DAG>
+__device__ __forceinline__ void project_biased(const float2 F[4][3], int mu, bool fwd, cx<float> h[2][3]) {
+  const float s = DAG ? -1.f : 1.f;
+  const float sg = fwd ? -s : s;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 0) {  // h0 = p0 + sg i p3, h1 = p1 + sg i p2
+      h[0][c] = mkc(comb_biased(F[0][c].x, F[3][c].y, 1.f, -sg), comb_biased(F[0][c].y, F[3][c].x, 1.f, sg));
+      h[1][c] = mkc(comb_biased(F[1][c].x, F[2][c].y, 1.f, -sg), comb_biased(F[1][c].y, F[2][c].x, 1.f, sg));
+    } else if (mu == 1) {  // h0 = p0 + sg p3, h1 = p1 - sg p2
+      h[0][c] = mkc(comb_biased(F[0][c].x, F[3][c].x, 1.f, sg), comb_biased(F[0][c].y, F[3][c].y, 1.f, sg));
+      h[1][c] = mkc(comb_biased(F[1][c].x, F[2][c].x, 1.f, -sg), comb_biased(F[1][c].y, F[2][c].y, 1.f, -sg));
+    } else {  // h0 = p0 + sg i p2, h1 = p1 - sg i p3
+      h[0][c] = mkc(comb_biased(F[0][c].x, F[2][c].y, 1.f, -sg), comb_biased(F[0][c].y, F[2][c].x, 1.f, sg));
+      h[1][c] = mkc(comb_biased(F[1][c].x, F[3][c].y, 1.f, sg), comb_biased(F[1][c].y, F[3][c].x, 1.f, -sg));
     }
   }
 }
@@ -662,51 +783,61 @@ __device__ __forceinline__ void mul_ud(const Link<R>& u, const cx<R> h[2][3], R 
     }
 }
 
-// b = sum over the 8 hops of the even/odd hopping term: out(parity e, site i)
-// from the field ``in`` of the opposite parity (d/D21.F90:29-77).
+// b = hscale * (sum over the 8 hops of the even/odd hopping term): out(parity
+// e, site i) from the field ``in`` of the opposite parity (d/D21.F90:29-77).
+// Every storage scale (int16 spinors and links), the boundary sign and hscale
+// are applied as one factor per hop, to the transported half spinor.
 template <Prec PS, Prec PG, bool DAG>
 __device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Site& st,
                                            const SpinorView<PS>& in, const GaugeView<PG>& U,
-                                           Spinor<typename SpinorView<PS>::R>& b) {
+                                           Spinor<typename SpinorView<PS>::R>& b,
+                                           typename SpinorView<PS>::R hscale = 1) {
   using R = typename SpinorView<PS>::R;
   const int o = 1 - e;
   zero(b);
 #pragma unroll
   for (int mu = 3; mu >= 0; mu--) {
-    // forward hop; the spinor's storage scale (int16 fields) is applied once
-    // to the transported half spinor, together with the boundary sign
+    // forward hop
     {
       int j = neighbour(g, st, i, mu, true);
       cx<R> h[2][3], f[2][3];
-      R sc;
+      R sc, lsc;
       if (mu == 3) {
         // (1 -+ gamma_4) keeps two spins: (3,4) for d, (1,2) for d_dag
         in.load_pair_raw(j, DAG ? 0 : 2, h, sc);
+      } else if constexpr (PS == Prec::F16) {
+        float2 F[4][3];
+        in.load_biased(j, F, sc);
+        project_biased<DAG>(F, mu, true, h);
       } else {
         Spinor<R> p;
         in.load_raw(j, p, sc);
         project<R, DAG>(p, mu, true, h);
       }
       Link<R> u;
-      U.load(mu, e, i, u);
-      mul_u(u, h, (R)hop_sign(g, st, mu, true) * sc, f);
+      U.load_raw(mu, e, i, u, lsc);
+      mul_u(u, h, (R)hop_sign(g, st, mu, true) * sc * lsc * hscale, f);
       recon_fwd<R, DAG>(b, mu, f);
     }
     // backward hop
     {
       int j = neighbour(g, st, i, mu, false);
       cx<R> h[2][3], f[2][3];
-      R sc;
+      R sc, lsc;
       if (mu == 3) {
         in.load_pair_raw(j, DAG ? 2 : 0, h, sc);
+      } else if constexpr (PS == Prec::F16) {
+        float2 F[4][3];
+        in.load_biased(j, F, sc);
+        project_biased<DAG>(F, mu, false, h);
       } else {
         Spinor<R> p;
         in.load_raw(j, p, sc);
         project<R, DAG>(p, mu, false, h);
       }
       Link<R> u;
-      U.load(mu, o, j, u);
-      mul_ud(u, h, (R)hop_sign(g, st, mu, false) * sc, f);
+      U.load_raw(mu, o, j, u, lsc);
+      mul_ud(u, h, (R)hop_sign(g, st, mu, false) * sc * lsc * hscale, f);
       recon_bwd<R, DAG>(b, mu, f);
     }
   }

@@ -283,10 +283,12 @@ struct KernelTimer {
     pending.push_back(e);
   }
   void end() { begin(); }
-  void collect() {
+  // nuse: how many of the recorded launches (in order) did work; launches
+  // queued after the solver stopped return at once and are left out
+  void collect(int nuse = 1 << 30) {
     if (!on) return;
     cudaStreamSynchronize(c->stream);
-    for (size_t k = 0; k + 1 < pending.size(); k += 2) {
+    for (size_t k = 0; k + 1 < pending.size() && (int)(k / 2) < nuse; k += 2) {
       float t = 0.f;
       cudaEventElapsedTime(&t, pending[k], pending[k + 1]);
       ms += t;
@@ -378,6 +380,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   const Geom& gs = geom_of(c, sloppy);  // stencil geometry (12-real FP64 links when SU(3))
   while (!h.done) {
     nl += 5 * batch;
+    const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
       // pass 1 (timed), pass 2 (+|M~p|^2 -> alpha), pass 3, pass 4 (+x,r update, |r|^2), p update
       kt.begin();
@@ -395,7 +398,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     CKL();
     int st = read_cg(c);
     if (st) return st;
-    kt.collect();
+    kt.collect(2 * (h.iter - iter0));  // two timed passes per iteration run
     if (batch < 16) batch *= 2;
     if (h.done == 4) break;
     if (h.done == 0) continue;
@@ -761,6 +764,7 @@ int bqcdg_create(bqcdg_ctx** out, const int L[4], const int bc[4], int device) {
   c->g.volh = (int)(vol / 2);
   c->g.stride = (c->g.volh + 63) / 64 * 64;
   c->g.rec12 = 0;
+  geom_finish(c->g);
   c->g12 = c->g;
   c->g12.rec12 = 1;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);

@@ -108,10 +108,11 @@ __global__ void __launch_bounds__(kBlock) k_gauge_demote32(Geom g, float4* out, 
     dst[k * g.stride] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
   }
 }
+// v in [-1, 1] -> offset-binary int16 q + 32768, q = round(32767 v)
 __device__ __forceinline__ short q16(double v) {
   double t = rint(v * 32767.0);
   t = fmin(32767.0, fmax(-32767.0, t));
-  return (short)t;
+  return (short)(unsigned short)((int)t + 32768);
 }
 __global__ void __launch_bounds__(kBlock) k_gauge_demote16(Geom g, short4* out, const double2* in) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -20,7 +20,7 @@ namespace bqcdg {
 #define BQCDG_SLOPPY_MIN_BLOCKS 6
 #endif
 #ifndef BQCDG_SLOPPY_MIN_BLOCKS2
-#define BQCDG_SLOPPY_MIN_BLOCKS2 5
+#define BQCDG_SLOPPY_MIN_BLOCKS2 4
 #endif
 template <Prec P>
 struct Occ {
@@ -210,13 +210,14 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
   Site st = site_coords(g, i, 1);
   Spinor<R> b;
   wilson_hop<P, P, DAG>(g, 1, i, st, in, U, b);
+  R osc = 1;  // a common factor of the output, folded into its storage scale
   if (has_clover) {
     Spinor<R> y;
-    clover_apply(cview<P>(ainv, g.stride), i, b, y);
+    clover_apply_raw(cview<P>(ainv, g.stride), i, b, y, osc);
     b = y;
   }
   if (hval != 0.0) h_mult_b(b, (R)hval);
-  out.store(i, b);
+  out.store_scaled(i, b, osc);
 }
 
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
@@ -233,31 +234,33 @@ void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorP
 
 // core of the second half: out = A_ee x + b D_eo t (clover) or x + b D_eo t
 // (+ i h' g5 x for Wilson, h_mult.F90:27-49), + rho x  (m_tilde.F90:63-73,
-// w_mult.F90:39)
+// w_mult.F90:39).  b is applied inside the hop sum and the storage scales of
+// x and A_ee as one factor, so no field is rescaled component by component.
 template <Prec P, bool DAG>
 __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorView<P>& t, const SpinorView<P>& xin,
                                            const GaugeView<P>& U, const CloverPtr& aee, int has_clover, double bcoef,
-                                           double hval, double rho, Spinor<typename SpinorView<P>::R>& out,
-                                           Spinor<typename SpinorView<P>::R>& x) {
+                                           double hval, double rho, Spinor<typename SpinorView<P>::R>& out) {
   using R = typename SpinorView<P>::R;
   Site st = site_coords(g, i, 0);
-  Spinor<R> hop;
-  wilson_hop<P, P, DAG>(g, 0, i, st, t, U, hop);
-  xin.load(i, x);
-  const R bb = (R)bcoef;
+  Spinor<R> hop, x;
+  wilson_hop<P, P, DAG>(g, 0, i, st, t, U, hop, (R)bcoef);
+  R xsc;
+  xin.load_raw(i, x, xsc);
   if (has_clover) {
-    clover_apply(cview<P>(aee, g.stride), i, x, out);
+    R csc;
+    clover_apply_raw(cview<P>(aee, g.stride), i, x, out, csc);
+    const R k = csc * xsc;
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) out.c[s][c] = out.c[s][c] + bb * hop.c[s][c];
+      for (int c = 0; c < 3; c++) out.c[s][c] = k * out.c[s][c] + hop.c[s][c];
   } else {
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) out.c[s][c] = x.c[s][c] + bb * hop.c[s][c];
+      for (int c = 0; c < 3; c++) out.c[s][c] = xsc * x.c[s][c] + hop.c[s][c];
     if (hval != 0.0) {
-      const R hh = (R)hval;
+      const R hh = (R)hval * xsc;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         out.c[0][c] = out.c[0][c] + hh * itimes(x.c[2][c]);
@@ -268,7 +271,7 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
     }
   }
   if (rho != 0.0) {
-    const R rr = (R)rho;
+    const R rr = (R)rho * xsc;
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
@@ -291,8 +294,8 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
     auto xin = sview<P>(rhs_of(xp, tl.rhs), g.stride);
     auto out = sview<P>(rhs_of(outp, tl.rhs), g.stride);
     auto U = gview<P>(gauge, g);
-    Spinor<R> o, x;
-    pass2_core<P, DAG>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o, x);
+    Spinor<R> o;
+    pass2_core<P, DAG>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o);
     out.store(i, o);
     if (REDUCE) {
 #pragma unroll
@@ -370,24 +373,26 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
     auto t = sview<P>(rhs_of(tp, tl.rhs), g.stride);
     auto q = sview<P>(rhs_of(qp, tl.rhs), g.stride);
     auto U = gview<P>(gauge, g);
-    Spinor<R> ap, qq;
-    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap, qq);
+    Spinor<R> ap;
+    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap);
     auto pv = sview<P>(rhs_of(pp, tl.rhs), g.stride);
     auto xv = sview<XP>(rhs_of(xp, tl.rhs), g.stride);
     auto rv = sview<XP>(rhs_of(rp, tl.rhs), g.stride);
     Spinor<R> pl;
-    pv.load(i, pl);
+    R psc;
+    pv.load_raw(i, pl, psc);
     Spinor<RX> xl, rl;
     xv.load(i, xl);
     rv.load(i, rl);
     const RX a = (RX)cg->alpha;
+    const RX ap_sc = a * (RX)psc;  // alpha and the storage scale of p
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         cx<RX> pc = mkc((RX)pl.c[s][c].x, (RX)pl.c[s][c].y);
         cx<RX> ac = mkc((RX)ap.c[s][c].x, (RX)ap.c[s][c].y);
-        xl.c[s][c] = xl.c[s][c] + a * pc;
+        xl.c[s][c] = xl.c[s][c] + ap_sc * pc;
         rl.c[s][c] = rl.c[s][c] - a * ac;
         acc[0] += (double)norm2(rl.c[s][c]);
       }
@@ -449,9 +454,10 @@ __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, Spi
   auto rv = sview<RP>(rhs_of(rp, tl.rhs), g.stride);
   Spinor<R> pl;
   Spinor<RR> rl;
-  pv.load(i, pl);
+  R psc;
+  pv.load_raw(i, pl, psc);
   rv.load(i, rl);
-  const R b = (R)cg->beta;
+  const R b = (R)cg->beta * psc;
 #pragma unroll
   for (int s = 0; s < 4; s++)
 #pragma unroll

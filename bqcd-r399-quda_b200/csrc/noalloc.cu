@@ -43,6 +43,7 @@ extern "C" int bqcdg_mdagm_noalloc(const int L[4], const int bc[4], const double
   g.volh = (int)(vol / 2);
   g.stride = (g.volh + 63) / 64 * 64;
   g.rec12 = 0;
+  geom_finish(g);
   if (g.stride > kMaxVolh) return BQCDG_EINVAL;
 
   // set-up, once per device and with that device current: the host-side
