@@ -399,6 +399,24 @@ __device__ __forceinline__ void reconstruct_col3(Link<R>& u) {
   u.m[2][2] = conjg(u.m[0][0] * u.m[1][1] - u.m[1][0] * u.m[0][1]);
 }
 
+// the three words of an int16 link (columns 1, 2; offset-binary) -> the link
+// times 32767 (U = u * lsc): the third column is rebuilt from the first two
+// and brought to the same scale, so one factor per hop replaces a multiply of
+// every entry
+__device__ __forceinline__ void links16_decode(uint2 t0, uint2 t1, uint2 t2, Link<float>& u, float& lsc) {
+  float2 e;
+  e = u16x2_to_f2(t0.x); u.m[0][0] = mkc(e.x, e.y);
+  e = u16x2_to_f2(t0.y); u.m[1][0] = mkc(e.x, e.y);
+  e = u16x2_to_f2(t1.x); u.m[2][0] = mkc(e.x, e.y);
+  e = u16x2_to_f2(t1.y); u.m[0][1] = mkc(e.x, e.y);
+  e = u16x2_to_f2(t2.x); u.m[1][1] = mkc(e.x, e.y);
+  e = u16x2_to_f2(t2.y); u.m[2][1] = mkc(e.x, e.y);
+  reconstruct_col3(u);  // 32767^2 times the true column
+  lsc = 1.0f / 32767.0f;
+#pragma unroll
+  for (int r = 0; r < 3; r++) u.m[r][2] = lsc * u.m[r][2];
+}
+
 template <Prec P>
 struct GaugeView;
 
@@ -434,6 +452,11 @@ struct GaugeView<Prec::F64> {
     load(mu, eo, i, u);
     lsc = 1.0;
   }
+  // the link of one hop: U_mu(idx) of parity eo (idx = the site for a
+  // forward hop, its backward neighbour for a backward one)
+  __device__ __forceinline__ void hop_link(int mu, bool, int eo, int idx, Link<double>& u, double& lsc) const {
+    load_raw(mu, eo, idx, u, lsc);
+  }
 };
 
 template <>
@@ -456,6 +479,11 @@ struct GaugeView<Prec::F32> {
     load(mu, eo, i, u);
     lsc = 1.0f;
   }
+  // the link of one hop: U_mu(idx) of parity eo (idx = the site for a
+  // forward hop, its backward neighbour for a backward one)
+  __device__ __forceinline__ void hop_link(int mu, bool, int eo, int idx, Link<float>& u, float& lsc) const {
+    load_raw(mu, eo, idx, u, lsc);
+  }
 };
 
 template <>
@@ -469,18 +497,10 @@ struct GaugeView<Prec::F16> {
   __device__ __forceinline__ void load_raw(int mu, int eo, int i, Link<float>& u, float& lsc) const {
     // one short4 = two complex entries = two 32-bit words
     const uint2* b = reinterpret_cast<const uint2*>(v) + (size_t)((mu * 2 + eo) * 3) * stride + i;
-    const uint2 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
-    float2 e;
-    e = u16x2_to_f2(t0.x); u.m[0][0] = mkc(e.x, e.y);
-    e = u16x2_to_f2(t0.y); u.m[1][0] = mkc(e.x, e.y);
-    e = u16x2_to_f2(t1.x); u.m[2][0] = mkc(e.x, e.y);
-    e = u16x2_to_f2(t1.y); u.m[0][1] = mkc(e.x, e.y);
-    e = u16x2_to_f2(t2.x); u.m[1][1] = mkc(e.x, e.y);
-    e = u16x2_to_f2(t2.y); u.m[2][1] = mkc(e.x, e.y);
-    reconstruct_col3(u);  // 32767^2 times the true column
-    lsc = 1.0f / 32767.0f;
-#pragma unroll
-    for (int r = 0; r < 3; r++) u.m[r][2] = lsc * u.m[r][2];
+    links16_decode(__ldg(b), __ldg(b + stride), __ldg(b + 2 * stride), u, lsc);
+  }
+  __device__ __forceinline__ void hop_link(int mu, bool, int eo, int idx, Link<float>& u, float& lsc) const {
+    load_raw(mu, eo, idx, u, lsc);
   }
   __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
     float lsc;
@@ -495,6 +515,20 @@ struct GaugeView<Prec::F16> {
 // clover blocks ------------------------------------------------------------
 // Packed 18-slot chiral block (clover.h:28-55): slot 0 = (A11,A22), 10 =
 // (A33,A44), 16 = (A55,A66) real diagonals; upper entries in slots 1-9,11-15,17.
+
+// word k (0..4) of chiral block chi of an int16 clover site (int4 number
+// chi*4 + k, 4 slots each) -> the slots of that block it holds, raw values
+__device__ __forceinline__ void clover16_decode(int chi, int k, int4 t, cx<float> a[18]) {
+  const unsigned w[4] = {(unsigned)t.x, (unsigned)t.y, (unsigned)t.z, (unsigned)t.w};
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int slot = 4 * (chi * 4 + k) + j - chi * 18;
+    if (slot >= 0 && slot < 18) {
+      const float2 e = u16x2_to_f2(w[j]);
+      a[slot] = mkc(e.x, e.y);
+    }
+  }
+}
 
 template <Prec P>
 struct CloverView;
@@ -554,19 +588,7 @@ struct CloverView<Prec::F16> {
   __device__ __forceinline__ void load_block_raw(int i, int chi, cx<float> a[18], float& sc) const {
     sc = __ldg(norm + i) * (1.0f / 32767.0f);
 #pragma unroll
-    for (int k = 0; k < 5; k++) {
-      const int word = chi * 4 + k;
-      const int4 t = __ldg(v + word * stride + i);
-      const unsigned w[4] = {(unsigned)t.x, (unsigned)t.y, (unsigned)t.z, (unsigned)t.w};
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int slot = 4 * word + j - chi * 18;
-        if (slot >= 0 && slot < 18) {
-          const float2 e = u16x2_to_f2(w[j]);
-          a[slot] = mkc(e.x, e.y);
-        }
-      }
-    }
+    for (int k = 0; k < 5; k++) clover16_decode(chi, k, __ldg(v + (chi * 4 + k) * stride + i), a);
   }
 };
 
@@ -605,9 +627,8 @@ __device__ __forceinline__ void clover_block_mv(const cx<R>* a, const cx<R> x[6]
 // blocks act on x+- = psi(spin 1,2) +- psi(spin 3,4).  The _raw form leaves
 // out = (A / sc) in, sc the storage scale of the site's blocks (1 except for
 // int16), for callers that fold sc into a later factor.
-template <Prec P, typename R>
-__device__ __forceinline__ void clover_apply_raw(const CloverView<P>& A, int i, const Spinor<R>& in, Spinor<R>& out,
-                                                 R& sc) {
+template <typename CV, typename R>
+__device__ __forceinline__ void clover_apply_raw(const CV& A, int i, const Spinor<R>& in, Spinor<R>& out, R& sc) {
   cx<R> x[6], y[6], a[18];
 #pragma unroll
   for (int k = 0; k < 6; k++) x[k] = in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3];
@@ -694,107 +715,120 @@ __device__ __forceinline__ void project_biased(const float2 F[4][3], int mu, boo
   }
 }
 
-// b += reconstruction of the transported forward half spinor f
-template <typename R, bool DAG>
-__device__ __forceinline__ void recon_fwd(Spinor<R>& b, int mu, const cx<R> f[2][3]) {
-  const R s = DAG ? R(-1) : R(1);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    if (mu == 3) {
-      if (!DAG) {
-        b.c[2][c] = b.c[2][c] + R(2) * f[0][c];
-        b.c[3][c] = b.c[3][c] + R(2) * f[1][c];
-      } else {
-        b.c[0][c] = b.c[0][c] + R(2) * f[0][c];
-        b.c[1][c] = b.c[1][c] + R(2) * f[1][c];
-      }
-    } else {
-      b.c[0][c] = b.c[0][c] + f[0][c];
-      b.c[1][c] = b.c[1][c] + f[1][c];
-      if (mu == 0) {
-        b.c[2][c] = b.c[2][c] + s * itimes(f[1][c]);
-        b.c[3][c] = b.c[3][c] + s * itimes(f[0][c]);
-      } else if (mu == 1) {
-        b.c[2][c] = b.c[2][c] + s * f[1][c];
-        b.c[3][c] = b.c[3][c] - s * f[0][c];
-      } else {
-        b.c[2][c] = b.c[2][c] + s * itimes(f[0][c]);
-        b.c[3][c] = b.c[3][c] - s * itimes(f[1][c]);
-      }
-    }
-  }
-}
-
-template <typename R, bool DAG>
-__device__ __forceinline__ void recon_bwd(Spinor<R>& b, int mu, const cx<R> f[2][3]) {
-  const R s = DAG ? R(-1) : R(1);
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    if (mu == 3) {
-      if (!DAG) {
-        b.c[0][c] = b.c[0][c] + R(2) * f[0][c];
-        b.c[1][c] = b.c[1][c] + R(2) * f[1][c];
-      } else {
-        b.c[2][c] = b.c[2][c] + R(2) * f[0][c];
-        b.c[3][c] = b.c[3][c] + R(2) * f[1][c];
-      }
-    } else {
-      b.c[0][c] = b.c[0][c] + f[0][c];
-      b.c[1][c] = b.c[1][c] + f[1][c];
-      if (mu == 0) {
-        b.c[2][c] = b.c[2][c] - s * itimes(f[1][c]);
-        b.c[3][c] = b.c[3][c] - s * itimes(f[0][c]);
-      } else if (mu == 1) {
-        b.c[2][c] = b.c[2][c] - s * f[1][c];
-        b.c[3][c] = b.c[3][c] + s * f[0][c];
-      } else {
-        b.c[2][c] = b.c[2][c] - s * itimes(f[0][c]);
-        b.c[3][c] = b.c[3][c] + s * itimes(f[1][c]);
-      }
-    }
-  }
-}
-
-// f = sgn * U h   (colour vectors h[0], h[1])
+// acc + a*f and acc + a*(i f): two FMAs each
 template <typename R>
-__device__ __forceinline__ void mul_u(const Link<R>& u, const cx<R> h[2][3], R sgn, cx<R> f[2][3]) {
+__device__ __forceinline__ cx<R> axpy_c(cx<R> acc, R a, cx<R> f) {
+  return mkc(fma(a, f.x, acc.x), fma(a, f.y, acc.y));
+}
+template <typename R>
+__device__ __forceinline__ cx<R> axpy_ic(cx<R> acc, R a, cx<R> f) {
+  return mkc(fma(-a, f.y, acc.x), fma(a, f.x, acc.y));
+}
+
+// b += k * (reconstruction of the transported forward half spinor f); k
+// carries the hop's boundary sign and storage scales, so applying it here
+// costs no instruction beyond the accumulation itself
+template <typename R, bool DAG>
+__device__ __forceinline__ void recon_fwd(Spinor<R>& b, int mu, const cx<R> f[2][3], R k) {
+  const R sk = DAG ? -k : k;
+  const R k2 = R(2) * k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 3) {
+      if (!DAG) {
+        b.c[2][c] = axpy_c(b.c[2][c], k2, f[0][c]);
+        b.c[3][c] = axpy_c(b.c[3][c], k2, f[1][c]);
+      } else {
+        b.c[0][c] = axpy_c(b.c[0][c], k2, f[0][c]);
+        b.c[1][c] = axpy_c(b.c[1][c], k2, f[1][c]);
+      }
+    } else {
+      b.c[0][c] = axpy_c(b.c[0][c], k, f[0][c]);
+      b.c[1][c] = axpy_c(b.c[1][c], k, f[1][c]);
+      if (mu == 0) {
+        b.c[2][c] = axpy_ic(b.c[2][c], sk, f[1][c]);
+        b.c[3][c] = axpy_ic(b.c[3][c], sk, f[0][c]);
+      } else if (mu == 1) {
+        b.c[2][c] = axpy_c(b.c[2][c], sk, f[1][c]);
+        b.c[3][c] = axpy_c(b.c[3][c], -sk, f[0][c]);
+      } else {
+        b.c[2][c] = axpy_ic(b.c[2][c], sk, f[0][c]);
+        b.c[3][c] = axpy_ic(b.c[3][c], -sk, f[1][c]);
+      }
+    }
+  }
+}
+
+// b += k * (reconstruction of the transported backward half spinor f)
+template <typename R, bool DAG>
+__device__ __forceinline__ void recon_bwd(Spinor<R>& b, int mu, const cx<R> f[2][3], R k) {
+  const R sk = DAG ? -k : k;
+  const R k2 = R(2) * k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if (mu == 3) {
+      if (!DAG) {
+        b.c[0][c] = axpy_c(b.c[0][c], k2, f[0][c]);
+        b.c[1][c] = axpy_c(b.c[1][c], k2, f[1][c]);
+      } else {
+        b.c[2][c] = axpy_c(b.c[2][c], k2, f[0][c]);
+        b.c[3][c] = axpy_c(b.c[3][c], k2, f[1][c]);
+      }
+    } else {
+      b.c[0][c] = axpy_c(b.c[0][c], k, f[0][c]);
+      b.c[1][c] = axpy_c(b.c[1][c], k, f[1][c]);
+      if (mu == 0) {
+        b.c[2][c] = axpy_ic(b.c[2][c], -sk, f[1][c]);
+        b.c[3][c] = axpy_ic(b.c[3][c], -sk, f[0][c]);
+      } else if (mu == 1) {
+        b.c[2][c] = axpy_c(b.c[2][c], -sk, f[1][c]);
+        b.c[3][c] = axpy_c(b.c[3][c], sk, f[0][c]);
+      } else {
+        b.c[2][c] = axpy_ic(b.c[2][c], -sk, f[0][c]);
+        b.c[3][c] = axpy_ic(b.c[3][c], sk, f[1][c]);
+      }
+    }
+  }
+}
+
+// f = U h   (colour vectors h[0], h[1])
+template <typename R>
+__device__ __forceinline__ void mul_u(const Link<R>& u, const cx<R> h[2][3], cx<R> f[2][3]) {
 #pragma unroll
   for (int k = 0; k < 2; k++)
 #pragma unroll
     for (int r = 0; r < 3; r++) {
       cx<R> t = u.m[r][0] * h[k][0];
       t = fma_c(t, u.m[r][1], h[k][1]);
-      t = fma_c(t, u.m[r][2], h[k][2]);
-      f[k][r] = sgn * t;
+      f[k][r] = fma_c(t, u.m[r][2], h[k][2]);
     }
 }
-// f = sgn * U^+ h
+// f = U^+ h
 template <typename R>
-__device__ __forceinline__ void mul_ud(const Link<R>& u, const cx<R> h[2][3], R sgn, cx<R> f[2][3]) {
+__device__ __forceinline__ void mul_ud(const Link<R>& u, const cx<R> h[2][3], cx<R> f[2][3]) {
 #pragma unroll
   for (int k = 0; k < 2; k++)
 #pragma unroll
     for (int r = 0; r < 3; r++) {
-      cx<R> t = mkc<R>(0, 0);
-      t = fma_cc(t, u.m[0][r], h[k][0]);
+      cx<R> t = mulc(h[k][0], u.m[0][r]);
       t = fma_cc(t, u.m[1][r], h[k][1]);
-      t = fma_cc(t, u.m[2][r], h[k][2]);
-      f[k][r] = sgn * t;
+      f[k][r] = fma_cc(t, u.m[2][r], h[k][2]);
     }
 }
 
-// b = hscale * (sum over the 8 hops of the even/odd hopping term): out(parity
+// b += hscale * (sum over the 8 hops of the even/odd hopping term): out(parity
 // e, site i) from the field ``in`` of the opposite parity (d/D21.F90:29-77).
+// b is accumulated into, so a caller either zeroes it or starts it with the
+// site-local terms of its operator.
 // Every storage scale (int16 spinors and links), the boundary sign and hscale
 // are applied as one factor per hop, to the transported half spinor.
-template <Prec PS, Prec PG, bool DAG>
+template <Prec PS, bool DAG, typename UV>
 __device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Site& st,
-                                           const SpinorView<PS>& in, const GaugeView<PG>& U,
+                                           const SpinorView<PS>& in, const UV& U,
                                            Spinor<typename SpinorView<PS>::R>& b,
                                            typename SpinorView<PS>::R hscale = 1) {
   using R = typename SpinorView<PS>::R;
   const int o = 1 - e;
-  zero(b);
 #pragma unroll
   for (int mu = 3; mu >= 0; mu--) {
     // forward hop
@@ -815,9 +849,9 @@ __device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Si
         project<R, DAG>(p, mu, true, h);
       }
       Link<R> u;
-      U.load_raw(mu, e, i, u, lsc);
-      mul_u(u, h, (R)hop_sign(g, st, mu, true) * sc * lsc * hscale, f);
-      recon_fwd<R, DAG>(b, mu, f);
+      U.hop_link(mu, true, e, i, u, lsc);
+      mul_u(u, h, f);
+      recon_fwd<R, DAG>(b, mu, f, (R)hop_sign(g, st, mu, true) * sc * lsc * hscale);
     }
     // backward hop
     {
@@ -836,9 +870,9 @@ __device__ __forceinline__ void wilson_hop(const Geom& g, int e, int i, const Si
         project<R, DAG>(p, mu, false, h);
       }
       Link<R> u;
-      U.load_raw(mu, o, j, u, lsc);
-      mul_ud(u, h, (R)hop_sign(g, st, mu, false) * sc * lsc * hscale, f);
-      recon_bwd<R, DAG>(b, mu, f);
+      U.hop_link(mu, false, o, j, u, lsc);
+      mul_ud(u, h, f);
+      recon_bwd<R, DAG>(b, mu, f, (R)hop_sign(g, st, mu, false) * sc * lsc * hscale);
     }
   }
 }

@@ -20,7 +20,7 @@ namespace bqcdg {
 #define BQCDG_SLOPPY_MIN_BLOCKS 6
 #endif
 #ifndef BQCDG_SLOPPY_MIN_BLOCKS2
-#define BQCDG_SLOPPY_MIN_BLOCKS2 4
+#define BQCDG_SLOPPY_MIN_BLOCKS2 5
 #endif
 template <Prec P>
 struct Occ {
@@ -86,7 +86,8 @@ __global__ void __launch_bounds__(kBlock) k_dslash(Geom g, int e, SpinorPtr outp
   auto U = gview<P>(gauge, g);
   Site st = site_coords(g, i, e);
   Spinor<R> b;
-  wilson_hop<P, P, DAG>(g, e, i, st, in, U, b);
+  zero(b);
+  wilson_hop<P, DAG>(g, e, i, st, in, U, b);
   out.store(i, b);
 }
 
@@ -209,7 +210,8 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
   auto U = gview<P>(gauge, g);
   Site st = site_coords(g, i, 1);
   Spinor<R> b;
-  wilson_hop<P, P, DAG>(g, 1, i, st, in, U, b);
+  zero(b);
+  wilson_hop<P, DAG>(g, 1, i, st, in, U, b);
   R osc = 1;  // a common factor of the output, folded into its storage scale
   if (has_clover) {
     Spinor<R> y;
@@ -234,18 +236,19 @@ void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorP
 
 // core of the second half: out = A_ee x + b D_eo t (clover) or x + b D_eo t
 // (+ i h' g5 x for Wilson, h_mult.F90:27-49), + rho x  (m_tilde.F90:63-73,
-// w_mult.F90:39).  b is applied inside the hop sum and the storage scales of
-// x and A_ee as one factor, so no field is rescaled component by component.
+// w_mult.F90:39).  The site-local terms come first and the hop sum is added
+// onto them, so the clover block and x are dead before the neighbour gathers
+// start; b is applied inside the hop sum and the storage scales of x and A_ee
+// as one factor, so no field is rescaled component by component.
 template <Prec P, bool DAG>
 __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorView<P>& t, const SpinorView<P>& xin,
                                            const GaugeView<P>& U, const CloverPtr& aee, int has_clover, double bcoef,
                                            double hval, double rho, Spinor<typename SpinorView<P>::R>& out) {
   using R = typename SpinorView<P>::R;
-  Site st = site_coords(g, i, 0);
-  Spinor<R> hop, x;
-  wilson_hop<P, P, DAG>(g, 0, i, st, t, U, hop, (R)bcoef);
+  Spinor<R> x;
   R xsc;
   xin.load_raw(i, x, xsc);
+  const R rr = (R)rho * xsc;
   if (has_clover) {
     R csc;
     clover_apply_raw(cview<P>(aee, g.stride), i, x, out, csc);
@@ -253,12 +256,13 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) out.c[s][c] = k * out.c[s][c] + hop.c[s][c];
+      for (int c = 0; c < 3; c++) out.c[s][c] = rho != 0.0 ? k * out.c[s][c] + rr * x.c[s][c] : k * out.c[s][c];
   } else {
+    const R k = xsc + rr;
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) out.c[s][c] = xsc * x.c[s][c] + hop.c[s][c];
+      for (int c = 0; c < 3; c++) out.c[s][c] = k * x.c[s][c];
     if (hval != 0.0) {
       const R hh = (R)hval * xsc;
 #pragma unroll
@@ -270,13 +274,8 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
       }
     }
   }
-  if (rho != 0.0) {
-    const R rr = (R)rho * xsc;
-#pragma unroll
-    for (int s = 0; s < 4; s++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) out.c[s][c] = out.c[s][c] + rr * x.c[s][c];
-  }
+  const Site st = site_coords(g, i, 0);
+  wilson_hop<P, DAG>(g, 0, i, st, t, U, out, (R)bcoef);
 }
 
 template <Prec P, bool DAG, bool REDUCE>
@@ -373,30 +372,37 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
     auto t = sview<P>(rhs_of(tp, tl.rhs), g.stride);
     auto q = sview<P>(rhs_of(qp, tl.rhs), g.stride);
     auto U = gview<P>(gauge, g);
-    Spinor<R> ap;
-    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap);
     auto pv = sview<P>(rhs_of(pp, tl.rhs), g.stride);
     auto xv = sview<XP>(rhs_of(xp, tl.rhs), g.stride);
     auto rv = sview<XP>(rhs_of(rp, tl.rhs), g.stride);
-    Spinor<R> pl;
-    R psc;
-    pv.load_raw(i, pl, psc);
-    Spinor<RX> xl, rl;
-    xv.load(i, xl);
-    rv.load(i, rl);
     const RX a = (RX)cg->alpha;
-    const RX ap_sc = a * (RX)psc;  // alpha and the storage scale of p
+    {
+      // x += alpha p first: alpha is known before the stencil, and x and p are
+      // then dead while the stencil runs
+      Spinor<R> pl;
+      R psc;
+      pv.load_raw(i, pl, psc);
+      Spinor<RX> xl;
+      xv.load(i, xl);
+      const RX ap_sc = a * (RX)psc;  // alpha and the storage scale of p
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          xl.c[s][c] = xl.c[s][c] + ap_sc * mkc((RX)pl.c[s][c].x, (RX)pl.c[s][c].y);
+      xv.store(i, xl);
+    }
+    Spinor<R> ap;
+    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap);
+    Spinor<RX> rl;
+    rv.load(i, rl);
 #pragma unroll
     for (int s = 0; s < 4; s++)
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        cx<RX> pc = mkc((RX)pl.c[s][c].x, (RX)pl.c[s][c].y);
-        cx<RX> ac = mkc((RX)ap.c[s][c].x, (RX)ap.c[s][c].y);
-        xl.c[s][c] = xl.c[s][c] + ap_sc * pc;
-        rl.c[s][c] = rl.c[s][c] - a * ac;
+        rl.c[s][c] = rl.c[s][c] - a * mkc((RX)ap.c[s][c].x, (RX)ap.c[s][c].y);
         acc[0] += (double)norm2(rl.c[s][c]);
       }
-    xv.store(i, xl);
     rv.store(i, rl);
   }
   double* part = red.partial + (size_t)tl.rhs * kRedVals * red.maxblocks;
