@@ -2,7 +2,8 @@
 
 Workload (the 32^3 x 64 configuration): clover-Wilson, c_sw = 1.9192,
 kappa = 0.13, antiperiodic in t; links = seeded hot start (BQCD's ranf, default
-seed) + 10 sweeps of conf_relax cooling, all generated on the device; b =
+seed) + conf_relax cooling sweeps until the plaquette reaches 0.55 (one sweep
+does it), all generated on the device; b =
 ran_gauss_volh(12, b, 1/2, EVEN) (unit-variance complex).  A step is one solve
 of M~^+M~ x = b from x = 0 to a true FP64 |r|/|b| < 1e-10:
   value   mixed-precision CG (int16 sloppy fields, FP64 reliable updates), s
@@ -173,6 +174,13 @@ def build_system(bq, L, device, seed_skip, cool):
     return lat, hb, hx
 
 
+# DRAM bytes (read + write) of one k_pass1<int16> launch per output site, from
+# one ncu capture at 32x32x32x32 (dram__bytes_read.sum + dram__bytes_write.sum
+# = 207.3 + 18.5 MB for 524288 sites); traffic grows with the number of
+# sites, so the per-launch figure at another volume is this times volh
+TRAFFIC_PER_SITE_INT16 = 430.6
+
+
 def stencil_bytes_per_site(prec):
     """Algorithmic bytes of one mtil first-half pass (D_oe + Ainv_oo) per odd
     output site: read the input spinor once, 8 links, one clover block, write
@@ -282,7 +290,7 @@ def run_ours(args):
                      "dslash_gbs": round(f64_gbs, 1), "dslash_frac": round(f64_gbs / peak, 4)},
             "speedup_mixed_vs_fp64": round(fp64_s / step_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(st_gbs, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(st_gbs / peak, 4), "traffic": None,
+                         "frac": round(st_gbs / peak, 4), "traffic": int(TRAFFIC_PER_SITE_INT16 * lat.volh),
                          "kernel": "k_pass1<F16> (D_oe + Ainv_oo, int16 fields)",
                          "bytes_per_launch": st_bytes, "avg_launch_ms": round(st_ms, 5), "peak_kind": peak_kind},
             "e2e": e2e,
