@@ -962,13 +962,28 @@ __device__ __forceinline__ bool last_block(unsigned int* counter, int nsb) {
 
 template <int N>
 __device__ __forceinline__ void final_sum(const double* partial, int nblocks_stride, int nsb, double (&out)[N]) {
-  // executed by the whole last block: warp-parallel fixed-order sum
+  // executed by the whole last block: warp-parallel fixed-order sum.  Each
+  // thread keeps 8 loads in flight (8 running sums, combined in a fixed
+  // order), so the tail that the rest of the GPU waits for costs a few L2
+  // latencies rather than one per partial.
   __shared__ double red[N][32];
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int k = 0; k < N; k++) {
-    double x = 0.0;
-    for (int b = threadIdx.x; b < nsb; b += blockDim.x) x += __ldcg(partial + k * nblocks_stride + b);
+    const double* p = partial + k * nblocks_stride;
+    double s[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int b = threadIdx.x;
+    for (; b + 7 * (int)blockDim.x < nsb; b += 8 * blockDim.x) {
+      double t[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) t[j] = __ldcg(p + b + j * blockDim.x);
+#pragma unroll
+      for (int j = 0; j < 8; j++) s[j] += t[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 7; j++)
+      if (b + j * (int)blockDim.x < nsb) s[j] += __ldcg(p + b + j * blockDim.x);
+    double x = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
     if (lane == 0) red[k][warp] = x;

@@ -392,8 +392,8 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
       launch_mtil_pass1(sloppy, gs, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
       kt.end();
       launch_cg_pass4(sloppy, gs, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
-                      c->stream);
-      launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream);
+                      c->stream, 1, false);
+      launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream, 1, xs, iter0 + k + 1);
     }
     CKL();
     int st = read_cg(c);

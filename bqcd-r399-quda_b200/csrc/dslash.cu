@@ -356,7 +356,7 @@ struct XR<Prec::F32> {
   using View = SpinorView<Prec::F32>;
 };
 
-template <Prec P, Prec XP>
+template <Prec P, Prec XP, bool XUPD>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
@@ -376,9 +376,9 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
     auto xv = sview<XP>(rhs_of(xp, tl.rhs), g.stride);
     auto rv = sview<XP>(rhs_of(rp, tl.rhs), g.stride);
     const RX a = (RX)cg->alpha;
-    {
+    if (XUPD) {
       // x += alpha p first: alpha is known before the stencil, and x and p are
-      // then dead while the stencil runs
+      // then dead while the stencil runs (otherwise k_cg_pupdate does it)
       Spinor<R> pl;
       R psc;
       pv.load_raw(i, pl, psc);
@@ -429,39 +429,56 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
 
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr) {
+                     cudaStream_t s, int nr, bool xupd) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = -op.h;  // mtil_dag
-  if (p == Prec::F64)
-    k_cg_pass4<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg, nr);
-  else if (p == Prec::F32)
-    k_cg_pass4<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg, nr);
-  else
-    k_cg_pass4<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec,
-                                                             x, r, red, cg, nr);
+#define P4(PP, XX, XU)                                                                                          \
+  k_cg_pass4<PP, XX, XU><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec, x, r, red, \
+                                                 cg, nr)
+  if (p == Prec::F64) { if (xupd) P4(Prec::F64, Prec::F64, true); else P4(Prec::F64, Prec::F64, false); }
+  else if (p == Prec::F32) { if (xupd) P4(Prec::F32, Prec::F32, true); else P4(Prec::F32, Prec::F32, false); }
+  else { if (xupd) P4(Prec::F16, Prec::F32, true); else P4(Prec::F16, Prec::F32, false); }
+#undef P4
 }
 
-// p = r + beta p   (sc_xpby, cg.F90:116)
-template <Prec P, Prec RP>
-__global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, SpinorPtr rp, const CgScalars* cgs,
-                                                       int nr) {
+// p = r + beta p   (sc_xpby, cg.F90:116), and, when x is given, the x += alpha p
+// of the same iteration (cg.F90:101), which then runs here instead of in the
+// stencil pass: this kernel reads p anyway.  The launch belongs to iteration
+// `expect`: x is updated iff that iteration ran (its k_cg_pass4 counted it),
+// p iff the solve goes on; so the update of the last iteration is not lost
+// when the solver stops, and no x update is applied twice.
+template <Prec P, Prec RP, bool XUPD>
+__global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, SpinorPtr rp, SpinorPtr xp,
+                                                       const CgScalars* cgs, int nr, int expect) {
   using R = typename SpinorView<P>::R;
   using RR = typename SpinorView<RP>::R;
   const Tile tl = tile(nr);
   const CgScalars* cg = cgs + tl.rhs;
-  if (cg->done) return;
+  const bool upd_p = !cg->done;
+  const bool upd_x = XUPD && cg->iter == expect;
+  if (!upd_p && !upd_x) return;
   const int i = tl.i;
   if (i >= g.volh) return;
   auto pv = sview<P>(rhs_of(pp, tl.rhs), g.stride);
-  auto rv = sview<RP>(rhs_of(rp, tl.rhs), g.stride);
   Spinor<R> pl;
-  Spinor<RR> rl;
   R psc;
   pv.load_raw(i, pl, psc);
+  if (XUPD && upd_x) {
+    auto xv = sview<RP>(rhs_of(xp, tl.rhs), g.stride);
+    Spinor<RR> xl;
+    xv.load(i, xl);
+    const RR a = (RR)cg->alpha * (RR)psc;
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) xl.c[s][c] = xl.c[s][c] + a * mkc((RR)pl.c[s][c].x, (RR)pl.c[s][c].y);
+    xv.store(i, xl);
+  }
+  if (!upd_p) return;
+  auto rv = sview<RP>(rhs_of(rp, tl.rhs), g.stride);
+  Spinor<RR> rl;
   rv.load(i, rl);
   const R b = (R)cg->beta * psc;
 #pragma unroll
@@ -471,11 +488,15 @@ __global__ void __launch_bounds__(kBlock) k_cg_pupdate(Geom g, SpinorPtr pp, Spi
   pv.store(i, pl);
 }
 
-void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s, int nr) {
+void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s, int nr,
+                       SpinorPtr x, int expect) {
   dim3 grid(nblocks(g.volh) * nr);
-  if (p == Prec::F64) k_cg_pupdate<Prec::F64, Prec::F64><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
-  else if (p == Prec::F32) k_cg_pupdate<Prec::F32, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
-  else k_cg_pupdate<Prec::F16, Prec::F32><<<grid, kBlock, 0, s>>>(g, pvec, r, cg, nr);
+  const bool xu = x.v != nullptr;
+#define PU(PP, RR, XU) k_cg_pupdate<PP, RR, XU><<<grid, kBlock, 0, s>>>(g, pvec, r, x, cg, nr, expect)
+  if (p == Prec::F64) { if (xu) PU(Prec::F64, Prec::F64, true); else PU(Prec::F64, Prec::F64, false); }
+  else if (p == Prec::F32) { if (xu) PU(Prec::F32, Prec::F32, true); else PU(Prec::F32, Prec::F32, false); }
+  else { if (xu) PU(Prec::F16, Prec::F32, true); else PU(Prec::F16, Prec::F32, false); }
+#undef PU
 }
 
 }  // namespace bqcdg

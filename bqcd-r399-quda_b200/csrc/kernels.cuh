@@ -87,10 +87,11 @@ void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorP
 // stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr = 1);
-// p = r + beta p
+                     cudaStream_t s, int nr = 1, bool xupd = true);
+// p = r + beta p; with x given (xupd = false above, single RHS), also the
+// x += alpha p of iteration `expect` if that iteration ran
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,
-                       int nr = 1);
+                       int nr = 1, SpinorPtr x = SpinorPtr{}, int expect = -1);
 
 // ---- BLAS / conversions (blas.cu) ----
 // r = b - Ax (F64), copy r into p (precision pp); res2[0] = |r|^2, res2[1] = |b|^2
