@@ -292,8 +292,14 @@ class Lattice:
         return x, it.value, info
 
     def solve(self, x, b, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000, delta=0.1,
-              time_kernels=False, rho=None):
-        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+              time_kernels=False, rho=None, inplace=False):
+        """x (initial guess) -> solution; a copy unless inplace, in which
+        case x must be a C-contiguous complex128 array (it may live in pinned
+        host memory, so that its transfers run at the link's rate)."""
+        if inplace:
+            _ptr(x, np.complex128)
+        else:
+            x = np.array(x, dtype=np.complex128, copy=True, order="C")
         o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, int(time_kernels))
         info = SolveInfo()
         prm = para.params(rho) if isinstance(para, HmcPara) else para
