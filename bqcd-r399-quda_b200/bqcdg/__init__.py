@@ -113,6 +113,23 @@ def _lib_handle():
         L.bqcdg_conf_relax.argtypes = [vp, i]
         L.bqcdg_sg.argtypes = [vp, P(C.c_double)]
         L.bqcdg_field_gauss.argtypes = [vp, i, C.c_double]
+        d, pd = C.c_double, P(C.c_double)
+        for n in ("bqcdg_mom_gauss", "bqcdg_mom_mark", "bqcdg_gauge_save"):
+            getattr(L, n).argtypes = [vp]
+        L.bqcdg_mom_set.argtypes = [vp, dp]
+        L.bqcdg_mom_get.argtypes = [vp, dp]
+        L.bqcdg_mom_action.argtypes = [vp, pd]
+        L.bqcdg_mom_change.argtypes = [vp, pd]
+        L.bqcdg_dsg_dev.argtypes = [vp, d, d]
+        L.bqcdg_hmc_u_dev.argtypes = [vp, d, d]
+        L.bqcdg_dsf_dev.argtypes = [vp, d, P(Params), i, i]
+        L.bqcdg_dsd_dev.argtypes = [vp, d, P(Params)]
+        L.bqcdg_gauge_restore.argtypes = [vp, d]
+        L.bqcdg_ranf.argtypes = [vp, pd]
+        L.bqcdg_op_dev.argtypes = [vp, i, i, i, P(Params)]
+        L.bqcdg_cg_dev.argtypes = [vp, i, i, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
+        L.bqcdg_field_cdot.argtypes = [vp, i, i, pd, pd]
+        L.bqcdg_field_caxpby.argtypes = [vp, i, d, d, d, i]
         _LIB = L
     return _LIB
 
@@ -371,6 +388,87 @@ class Lattice:
 
     def field_set(self, handle, host):
         _check(lib().bqcdg_field_upload(self.h, handle, _ptr(host, np.complex128)), "field_upload")
+
+    def field_cdot(self, ha, hb):
+        """<a, b> = sum conj(a) b of two resident fields."""
+        re, im = C.c_double(), C.c_double()
+        _check(lib().bqcdg_field_cdot(self.h, ha, hb, C.byref(re), C.byref(im)), "field_cdot")
+        return complex(re.value, im.value)
+
+    def field_caxpby(self, hy, ay, a, hx):
+        """y = ay y + a x (a complex) on resident fields."""
+        a = complex(a)
+        _check(lib().bqcdg_field_caxpby(self.h, hy, float(ay), a.real, a.imag, hx), "field_caxpby")
+
+    def field_copy(self, hdst, hsrc):
+        self.field_caxpby(hdst, 0.0, 1.0, hsrc)
+
+    OPS = {"mtil": 0, "mtil_dag": 1, "mtdagmt": 2, "w_mult": 3, "w_mult_dag": 4, "w_dagger_w": 5}
+
+    def op_dev(self, which, hout, hin, para, rho=None):
+        """hout = op(hin) on resident fields, op one of OPS (m_tilde.F90, w_mult.F90)."""
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_op_dev(self.h, self.OPS[which], hout, hin, C.byref(prm)), "op_dev")
+
+    def cg_dev(self, hx, hb, para, rest, maxiter=1000, log=0, rho=None):
+        """cg.F90 on resident fields (x: initial guess in, solution out);
+        returns (iterations, info)."""
+        it = C.c_int()
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        cp = CgPara(rest, maxiter, log)
+        _check(lib().bqcdg_cg_dev(self.h, hx, hb, C.byref(prm), C.byref(cp), C.byref(it), C.byref(info)), "cg_dev")
+        return it.value, info
+
+    # ---- resident HMC pieces (momenta, gauge update and force) ----
+    def mom_gauss(self):
+        _check(lib().bqcdg_mom_gauss(self.h), "mom_gauss")
+
+    def mom_set(self, p):
+        _check(lib().bqcdg_mom_set(self.h, _ptr(p, np.float64)), "mom_set")
+
+    def mom_get(self):
+        p = np.zeros((4, 2, self.volh, 8), np.float64)
+        _check(lib().bqcdg_mom_get(self.h, p.ctypes.data), "mom_get")
+        return p
+
+    def mom_action(self):
+        v = C.c_double()
+        _check(lib().bqcdg_mom_action(self.h, C.byref(v)), "mom_action")
+        return v.value
+
+    def mom_mark(self):
+        _check(lib().bqcdg_mom_mark(self.h), "mom_mark")
+
+    def mom_change(self):
+        v = C.c_double()
+        _check(lib().bqcdg_mom_change(self.h, C.byref(v)), "mom_change")
+        return v.value
+
+    def dsg_dev(self, step, beta):
+        _check(lib().bqcdg_dsg_dev(self.h, step, beta), "dsg_dev")
+
+    def hmc_u_dev(self, step, csw_kappa):
+        _check(lib().bqcdg_hmc_u_dev(self.h, step, csw_kappa), "hmc_u_dev")
+
+    def dsf_dev(self, step, para, ha, hb):
+        prm = para.params() if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_dsf_dev(self.h, step, C.byref(prm), ha, hb), "dsf_dev")
+
+    def dsd_dev(self, step, para):
+        prm = para.params() if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_dsd_dev(self.h, step, C.byref(prm)), "dsd_dev")
+
+    def gauge_save(self):
+        _check(lib().bqcdg_gauge_save(self.h), "gauge_save")
+
+    def gauge_restore(self, csw_kappa):
+        _check(lib().bqcdg_gauge_restore(self.h, csw_kappa), "gauge_restore")
+
+    def ranf(self):
+        v = C.c_double()
+        _check(lib().bqcdg_ranf(self.h, C.byref(v)), "ranf")
+        return v.value
 
     def solve_dev(self, hx, hb, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000, delta=0.1,
                   time_kernels=False, rho=None):

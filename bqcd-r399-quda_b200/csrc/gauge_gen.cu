@@ -110,36 +110,6 @@ __device__ __forceinline__ void store_link(const Geom& g, double2* gauge, int mu
     for (int r = 0; r < 3; r++) b[(c * 3 + r) * g.stride] = make_double2(u.m[r][c].x, u.m[r][c].y);
 }
 
-// staple.F90:28-63: sum over nu != mu of the forward and backward staples
-__device__ void staple(const Geom& g, const double2* gauge, const int x[4], int mu, L64& st) {
-  lzero(st);
-  for (int nu = 0; nu < 4; nu++) {
-    if (nu == mu) continue;
-    int x1[4], x2[4], x3[4], x4[4];
-    shift(g, x, mu, 1, x1);
-    shift(g, x, nu, 1, x2);
-    shift(g, x, nu, -1, x3);
-    shift(g, x3, mu, 1, x4);
-    L64 a, b, c, t, r;
-    // uuu_fwd: U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
-    load_link(g, gauge, nu, x1, a);
-    load_link(g, gauge, mu, x2, b);
-    load_link(g, gauge, nu, x, c);
-    mul2(t, a, false, b, true);
-    mul2(r, t, false, c, true);
-    for (int p = 0; p < 3; p++)
-      for (int q = 0; q < 3; q++) st.m[p][q] = st.m[p][q] + r.m[p][q];
-    // uuu_bwd: U_nu(x-nu+mu)^+ U_mu(x-nu)^+ U_nu(x-nu)
-    load_link(g, gauge, nu, x4, a);
-    load_link(g, gauge, mu, x3, b);
-    load_link(g, gauge, nu, x3, c);
-    mul2(t, a, true, b, true);
-    mul2(r, t, false, c, false);
-    for (int p = 0; p < 3; p++)
-      for (int q = 0; q < 3; q++) st.m[p][q] = st.m[p][q] + r.m[p][q];
-  }
-}
-
 __global__ void __launch_bounds__(128) k_conf_relax(Geom g, double2* gauge, int mu, int eo) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.volh) return;

@@ -162,4 +162,16 @@ void launch_cold(double2* u_fortran, long long nlinks, cudaStream_t s);
 void launch_conf_relax(const Geom& g, double2* gauge, cudaStream_t s);
 void launch_plaquette(const Geom& g, const double2* gauge, RedScratch red, double* out, cudaStream_t s);
 
+// ---- resident HMC pieces (hmc.cu) ----
+// U <- exp(i step p) U on every link, re-unitarised (hmc_u.F90:53-67)
+void launch_hmc_u(const Geom& g, double2* gauge, const double* p, double step, cudaStream_t s);
+// p += s Im Tr(lambda_j U staples) (dsg.F90:28-53), s = -step beta / 3
+void launch_dsg(const Geom& g, const double2* gauge, double* p, double s, cudaStream_t st);
+// sum over the momentum field of (a - b)^2, or a^2 when b is null
+void launch_mom_sumsq(const Geom& g, const double* a, const double* b, RedScratch red, double* out, cudaStream_t s);
+// out[0] + i out[1] = <a, b> of F64 spinors
+void launch_cdot(const Geom& g, const double2* a, const double2* b, RedScratch red, double* out, cudaStream_t s);
+// y = ay y + (are + i aim) x
+void launch_caxpby(const Geom& g, double are, double aim, const double2* x, double ay, double2* y, cudaStream_t s);
+
 }  // namespace bqcdg

@@ -209,6 +209,51 @@ int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, in
  * Ainv_oo) at the given precision, n launches */
 int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precision, int n, double *ms);
 
+/* ---- resident HMC pieces ------------------------------------------------ */
+/* With these a trajectory keeps the links, the momenta and its spinor fields
+ * in device memory: nothing crosses PCIe between the start and the
+ * accept/reject step.  Momenta are one device field per context in BQCD's
+ * GENERATOR_FIELD layout, real(8, volh, 0:1, 4) (defs.h:71); spinor fields
+ * are the resident handles above. */
+/* hmc_init_p.F90:28-45: momenta from ran_gauss_volh(4, p(:,:,eo,mu), 1, eo),
+ * mu outer, eo inner, from the context's RNG stream */
+int bqcdg_mom_gauss(bqcdg_ctx *ctx);
+int bqcdg_mom_set(bqcdg_ctx *ctx, const double *p);
+int bqcdg_mom_get(bqcdg_ctx *ctx, double *p);
+/* kinetic term of the Hamiltonian, sp = 1/2 sum p^2 (action.F90) */
+int bqcdg_mom_action(bqcdg_ctx *ctx, double *sp);
+/* force monitor (hmc_forces.F90:65-104): mark saves p, change returns
+ * sum (p_marked - p)^2 */
+int bqcdg_mom_mark(bqcdg_ctx *ctx);
+int bqcdg_mom_change(bqcdg_ctx *ctx, double *d2);
+/* dsg.F90:28-53: gauge force p += (-step beta / 3) Im Tr(lambda_j U staples) */
+int bqcdg_dsg_dev(bqcdg_ctx *ctx, double step, double beta);
+/* hmc_u.F90:28-69: U <- exp(i step p) U (gen2u, su3.F90:28-193), u_normalize,
+ * then clover_init of the new links when csw_kappa != 0 */
+int bqcdg_hmc_u_dev(bqcdg_ctx *ctx, double step, double csw_kappa);
+/* dsf.F90:28-110 into the resident momenta from resident fields a, b */
+int bqcdg_dsf_dev(bqcdg_ctx *ctx, double step, const bqcdg_params *p, int ha, int hb);
+/* dsd.F90:28-49: det-term force clover_dsd(ODD, p, b, -2 step csw_kappa/8) */
+int bqcdg_dsd_dev(bqcdg_ctx *ctx, double step, const bqcdg_params *p);
+/* links saved on the device and restored on a rejected trajectory
+ * (hmc.F90:195-199); restore rebuilds the clover when csw_kappa != 0 */
+int bqcdg_gauge_save(bqcdg_ctx *ctx);
+int bqcdg_gauge_restore(bqcdg_ctx *ctx, double csw_kappa);
+/* the next ranf() of the context's stream (ranf.F90), for the Metropolis step */
+int bqcdg_ranf(bqcdg_ctx *ctx, double *r);
+/* operators on resident fields: which = 0 mtil, 1 mtil_dag, 2 mtdagmt,
+ * 3 w_mult, 4 w_mult_dag, 5 w_dagger_w (m_tilde.F90:43-114, mtdagmt.F90:28,
+ * w_mult.F90:28-84) */
+int bqcdg_op_dev(bqcdg_ctx *ctx, int which, int hout, int hin, const bqcdg_params *p);
+/* cg(matrix_mult, x, b, para, conf, iterations) (cg.F90:51-137) on resident
+ * fields: FP64, the operator fixed by p->rho as in bqcdg_cg */
+int bqcdg_cg_dev(bqcdg_ctx *ctx, int hx, int hb, const bqcdg_params *p, const bqcdg_cg_para *cgp, int *iterations,
+                 bqcdg_solve_info *info);
+/* <a, b> = sum conj(a) b (sc_cdotc, sc.F90:224-286) and y = ay y + a x with
+ * complex a (the linear combinations of mre.F90:68-213) on resident fields */
+int bqcdg_field_cdot(bqcdg_ctx *ctx, int ha, int hb, double *re, double *im);
+int bqcdg_field_caxpby(bqcdg_ctx *ctx, int hy, double ay, double are, double aim, int hx);
+
 /* ---- allocation-free operator ------------------------------------------- */
 /* This entry point has no counterpart in the reference.  It is for callers
  * that cannot let the library allocate device memory: a framework whose pool

@@ -1,0 +1,145 @@
+"""The resident HMC pieces against the oracle, and one device trajectory
+against the reference's golden quick-test record.
+
+Links are stored [col][row] (Fortran u(row,col)), so a stored block is the
+transposed matrix: U -> G U reads u_stored -> u_stored @ g_stored, with
+g_stored the transposed gen2u as the oracle returns it.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+L = (4, 4, 4, 4)
+BC = (1, 1, 1, -1)
+
+
+@pytest.fixture
+def pair(oracle, bq):
+    g = oracle.Geom(L, BC)
+    oracle.ranset(11)
+    u = g.hot()
+    g.relax(u, 1)
+    lat = bq.Lattice(L, BC)
+    lat.load_gauge(u, flipped=False)
+    yield g, u, lat
+    lat.close()
+
+
+def test_momentum_draw_and_kinetic_term(oracle, bq, pair):
+    g, u, lat = pair
+    oracle.ranset(99)
+    p_ref = g.gauss_momenta()
+    lat.ranset(99)
+    lat.mom_gauss()
+    # same random stream exactly; the Box-Muller transcendentals of the
+    # device and the host libm differ in the last bits
+    assert np.abs(lat.mom_get() - p_ref).max() <= 1e-13
+    assert lat.ranget() == oracle.ranget()
+    assert abs(lat.mom_action() - 0.5 * np.sum(p_ref ** 2)) <= 1e-13 * np.sum(p_ref ** 2)
+
+
+def test_gauge_update_matches_gen2u(oracle, bq, pair):
+    g, u, lat = pair
+    rng = np.random.default_rng(3)
+    p = rng.standard_normal((4, 2, g.volh, 8))
+    step = 0.07
+    lat.mom_set(p)
+    lat.hmc_u_dev(step, 0.0)
+    got = lat.get_gauge(flipped=False)
+    want = np.empty_like(u)
+    for mu in range(4):
+        for eo in range(2):
+            for i in range(g.volh):
+                want[mu, eo, i] = u[mu, eo, i] @ oracle.gen2u(step * p[mu, eo, i])
+    assert np.abs(got - want).max() < 1e-13
+    # unitary to rounding after u_normalize
+    m = np.swapaxes(got, -1, -2)
+    eye = np.eye(3)
+    assert np.abs(m @ np.conj(np.swapaxes(m, -1, -2)) - eye).max() < 1e-14
+
+
+def test_gauge_force_matches_oracle(oracle, bq, pair):
+    g, u, lat = pair
+    rng = np.random.default_rng(5)
+    p = rng.standard_normal((4, 2, g.volh, 8))
+    lat.mom_set(p)
+    lat.dsg_dev(0.1, 5.29)
+    want = g.dsg(p.copy(), u, 0.1, 5.29)
+    got = lat.mom_get()
+    assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+
+
+def test_resident_forces_and_ops_match_host_entry_points(oracle, bq, pair):
+    g, u, lat = pair
+    para = bq.HmcPara(kappa=0.13, csw=1.9192, rho=0.1)
+    lat.clover_init(para.csw_kappa)
+    a, b = g.gauss_spinor(0), g.gauss_spinor(0)
+    p = np.random.default_rng(8).standard_normal((4, 2, g.volh, 8))
+    want = lat.dsf(p.copy(), 0.3, para, a, b)
+    ha, hb, hc = lat.field(a), lat.field(b), lat.field()
+    lat.mom_set(p)
+    lat.dsf_dev(0.3, para, ha, hb)
+    assert np.abs(lat.mom_get() - want).max() <= 1e-13 * np.abs(want).max()
+    want = lat.clover_dsd(1, p.copy(), -2 * 0.3 * para.csw_kappa / 8)
+    lat.mom_set(p)
+    lat.dsd_dev(0.3, para)
+    assert np.abs(lat.mom_get() - want).max() <= 1e-13 * np.abs(want).max()
+    for name in ("mtil", "mtil_dag", "mtdagmt", "w_mult", "w_mult_dag", "w_dagger_w"):
+        lat.op_dev(name, hc, ha, para)
+        ref = getattr(lat, name)(a, para)
+        assert np.linalg.norm(lat.field_get(hc) - ref) <= 1e-14 * np.linalg.norm(ref), name
+    z = lat.field_cdot(ha, hb)
+    zr = np.vdot(a, b)
+    assert abs(z - zr) <= 1e-13 * abs(zr)
+    lat.field_caxpby(hc, 0.5, 0.25 - 2j, ha)
+    ref = 0.5 * lat.w_dagger_w(a, para) + (0.25 - 2j) * a
+    assert np.linalg.norm(lat.field_get(hc) - ref) <= 1e-14 * np.linalg.norm(ref)
+
+
+def test_resident_cg_matches_reference_cg(oracle, bq, pair):
+    g, u, lat = pair
+    para = bq.HmcPara(kappa=0.13, csw=1.9192, rho=0.1)
+    lat.clover_init(para.csw_kappa)
+    uf = g.flip_bc(u.copy())
+    clov = g.clover_init(u, para.csw_kappa)
+    bvec = g.gauss_spinor(0)
+    x_ref, it_ref, _, rc = g.cg("w_dagger_w", np.zeros_like(bvec), bvec, uf, clov, 0.13, para.csw_kappa,
+                                rho=0.1, rest=1e-10)
+    hx, hb = lat.field(np.zeros_like(bvec)), lat.field(bvec)
+    it, info = lat.cg_dev(hx, hb, para, 1e-10)
+    assert rc == 0 and info.converged and abs(it - it_ref) <= 1
+    assert np.linalg.norm(lat.field_get(hx) - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+
+
+def test_quick_test_trajectory_on_device(bq):
+    """work/out.quick-test.reference: one 4^4 model-C trajectory (Hasenbusch
+    rho 0.1, kappa 0.13, c_sw 2.3327, beta 5.0, tau 0.2 in 10 steps of 3 inner
+    steps, MRE with 7 vectors, CG to rtr <= 1e-5) from a cold start with the
+    default seed, forced accept: every printed digit of the iteration counts, the
+    force monitors, the plaquette, exp(-dH) and the final RNG seed."""
+    from bqcdg.hmc import Hmc
+    with open(os.path.join(HERE, "golden", "quick_test.json")) as f:
+        gold = json.load(f)
+    lat = bq.Lattice(L, BC)
+    try:
+        lat.ranset(0)
+        lat.conf_cold()
+        hmc = Hmc(lat, beta=5.0, kappa=0.13, csw=2.3327, rho=0.1, traj_length=0.2, ntau=10, m_scale=3,
+                  model="C", rest=1e-5, maxiter=1000, mre_n_vec=7)
+        rec = hmc.trajectory(force_accept=True)
+        assert (rec["it_f1"], rec["it_f2"]) == (gold["it"]["f1"], gold["it"]["f2"]), rec
+        for key, got in (("Favg", rec["f_avg"]), ("Fmax", rec["f_max"])):
+            for a, b in zip(got, gold[key]["values"]):
+                assert abs(a - b) <= 6e-10 * abs(b), (key, a, b)
+        assert abs(rec["plaq_energy"] - gold["fa"]["plaq_energy"]) <= 6e-11
+        assert abs(rec["exp_dh"] - gold["fa"]["exp_mdh"]) <= 6e-11
+        assert (rec["cg_calls"], rec["cg_it_tot"], rec["cg_it_max"]) == \
+            (gold["fa"]["cg_calls"], gold["fa"]["cg_it_tot"], gold["fa"]["cg_it_max"])
+        assert lat.ranget() == gold["final_seed"]
+    finally:
+        lat.close()
