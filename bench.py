@@ -406,12 +406,68 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_hmc(args):
+    """Optional workload: full HMC trajectories at 24^3x48 (clover-Wilson
+    N_f = 2, Hasenbusch with two pseudofermions: kappa 0.1355, shift kappa
+    0.13 as rho = kappa/kappa_shift - 1 in BQCD's W = M~ + rho; beta 5.29,
+    c_sw 1.9192; trajectory length 1 in 20 outer x 5 inner leapfrog steps,
+    BQCD's only integrator; mixed-precision solves), every field resident on
+    the device.  The synthetic start (hot start + cooling) is brought towards
+    equilibrium by forced-accept pure-gauge trajectories first.  One step =
+    one trajectory; the value is seconds per trajectory."""
+    import numpy as np
+    import bqcdg as bq
+    from bqcdg.hmc import Hmc, quenched_trajectory
+
+    world, rank, local, pg = dist_init()
+    L = tuple(int(x) for x in (args.lattice if args.lattice != "32,32,32,64" else "24,24,24,48").split(","))
+    kappa, kshift, beta = 0.1355, 0.13, 5.29
+    lat, hb, _ = build_system(bq, L, local, 1000003 * rank, args.cool)
+    therm = []
+    for _ in range(args.therm):
+        acc, dh, plaq = quenched_trajectory(lat, beta, 1.0, 50, force_accept=True)
+        therm.append(round(plaq, 5))
+    b2 = lat.field_cdot(hb, hb).real   # |phi|^2 scale of a unit-variance field
+    hmc = Hmc(lat, beta=beta, kappa=kappa, csw=CSW, rho=kappa / kshift - 1, traj_length=1.0, ntau=20, m_scale=5,
+              model="C", rest=1e-20 * b2, maxiter=100000, solver="mixed")
+    recs = []
+    for k in range(args.warmup + args.steps):
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        rec = hmc.trajectory()
+        rec["seconds"] = allmax(pg, time.perf_counter() - t0, local)
+        if k >= args.warmup:
+            recs.append(rec)
+    if rank == 0:
+        secs = [r["seconds"] for r in recs]
+        out = {"metric": "HMC trajectory time at 24^3x48 (N_f=2 clover, Hasenbusch, 20/5 nested leapfrog)",
+               "value": round(sum(secs) / len(secs), 3), "unit": "s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 1),
+               "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64 (int16/f32 sloppy solves)", "data": "synthetic: hot start + %d conf_relax sweep(s), "
+               "then %d forced-accept pure-gauge trajectories (plaquettes %s)" % (lat.sweeps, args.therm, therm),
+               "config": {"workload": "HMC model C, lattice %s, kappa %.4f, kappa_shift %.2f (rho %.5f), c_sw %.4f, "
+                                      "beta %.2f, tau 1, 20x5 steps" % ("x".join(map(str, L)), kappa, kshift,
+                                                                      kappa / kshift - 1, CSW, beta),
+                          "parallelism": "replicas x%d" % world},
+               "trajectories": [{k: r[k] for k in ("accepted", "dh", "plaq_energy", "it_f1", "it_f2", "cg_calls",
+                                                   "cg_it_max", "seconds")} for r in recs],
+               "acceptance": sum(1 for r in recs if r["accepted"]) / len(recs)}
+        print(json.dumps(out))
+    lat.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="solve", choices=["solve", "hmc"],
+                    help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories")
+    ap.add_argument("--therm", type=int, default=10, help="hmc: forced-accept pure-gauge trajectories first")
     ap.add_argument("--lattice", default="32,32,32,64")
     ap.add_argument("--cool", type=int, default=-1,
                     help="conf_relax sweeps; -1: until the plaquette reaches %.2f" % PLAQ_TARGET)
@@ -425,6 +481,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "hmc":
+        run_hmc(args)
     else:
         run_ours(args)
 

@@ -132,12 +132,15 @@ class Hmc:
     pseudofermion, or two with Hasenbusch's W = M~ + rho) on one Lattice.
 
     beta, kappa, csw, rho, traj_length, ntau, m_scale, model as in BQCD's
-    input (tau = traj_length / ntau, bqcd.F90:175).  Solves use the FP64 CG of
-    cg.F90 with its absolute stopping rule rtr <= rest; a solver that does
-    not converge raises, as cg.F90 dies unless log == 2."""
+    input (tau = traj_length / ntau, bqcd.F90:175).  Solves stop on BQCD's
+    absolute rule rtr <= rest.  solver = "cg" is the FP64 CG of cg.F90;
+    "mixed" is the path of BQCD's QUDA hook (invert_quda.F90): int16 sloppy
+    iterations with FP64 reliable updates, the stop checked on the true FP64
+    residual.  A solver that does not converge raises, as cg.F90 dies unless
+    log == 2."""
 
     def __init__(self, lat, beta, kappa, csw, rho, traj_length, ntau, m_scale, model="C", rest=1e-5,
-                 maxiter=1000, mre_n_vec=7):
+                 maxiter=1000, mre_n_vec=7, solver="cg"):
         self.lat = lat
         self.beta = beta
         self.para = HmcPara(kappa=kappa, csw=csw, rho=rho)
@@ -149,6 +152,9 @@ class Hmc:
         self.hasenbusch = model != "A"
         self.rest = rest
         self.maxiter = maxiter
+        if solver not in ("cg", "mixed"):
+            raise ValueError("solver must be 'cg' or 'mixed'")
+        self.solver = solver
         self.phi = lat.field()
         self.phi2 = lat.field()
         self.phi_bck = lat.field()
@@ -164,7 +170,15 @@ class Hmc:
     # ---- solver and monitors ----
     def _solve(self, op, hx, hb):
         rho = self.para.rho if op == "w_dagger_w" else 0.0
-        it, _ = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=0, rho=rho)
+        if self.solver == "cg":
+            it, _ = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=0, rho=rho)
+        else:
+            from . import PREC_HALF
+            info = self.lat.solve_dev(hx, hb, self.para, precision=PREC_HALF, tol=self.rest, relative=False,
+                                      maxiter=self.maxiter, rho=rho)
+            if not info.converged:
+                raise RuntimeError("mixed-precision solve did not converge: %s" % info.as_dict())
+            it = info.niter
         self.cg_ncall += 1
         self.cg_niter_tot += it
         self.cg_niter_max = max(self.cg_niter_max, it)
@@ -316,3 +330,25 @@ class Hmc:
             "f_avg": [a / c if c else a for a, c in zip(self.f_avg, self.f_count)],
             "f_max": list(self.f_max),
         }
+
+
+def quenched_trajectory(lat, beta, traj_length, nsteps, force_accept=False):
+    """One pure-gauge HMC trajectory (BQCD with no fermions: the gauge force
+    of dsg.F90 in a plain leapfrog of nsteps, hmc_u.F90 updates), for
+    bringing a synthetic start configuration to equilibrium at beta before
+    dynamical trajectories.  Returns (accepted, dH, plaquette <Re Tr P>/3)."""
+    dt = traj_length / nsteps
+    lat.gauge_save()
+    lat.mom_gauss()
+    h_old = lat.mom_action() + beta * lat.sg()
+    lat.dsg_dev(0.5 * dt, beta)
+    for k in range(nsteps):
+        lat.hmc_u_dev(dt, 0.0)
+        lat.dsg_dev(dt if k < nsteps - 1 else 0.5 * dt, beta)
+    sg = lat.sg()
+    dh = lat.mom_action() + beta * sg - h_old
+    accepted = force_accept or lat.ranf() < math.exp(-dh)
+    if not accepted:
+        lat.gauge_restore(0.0)
+        sg = lat.sg()
+    return accepted, dh, 1.0 - sg / (6.0 * 2 * lat.volh)

@@ -306,6 +306,10 @@ constexpr int kStalled = 100;  // internal: the sloppy precision stopped converg
 // a reliable update at least every kRuEvery sloppy iterations, so that a
 // stagnating true residual is seen even when the iterated one keeps falling
 constexpr int kRuEvery = 1000;
+// int16 iterations get the shorter period: two periodic updates in a row
+// (the iterated residual could not fall by delta within it) show that int16
+// has run out of accuracy for the system, and the solve moves to FP32
+constexpr int kRuEvery16 = 500;
 
 // Core CG on device-resident x, b (F64, device layout).  Solves (W^+W) x = b.
 //   sloppy == F64: plain FP64 CG (cg.F90)
@@ -366,10 +370,11 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   h.maxiter = maxiter;
   h.delta2 = sloppy == Prec::F64 ? 0.0 : delta * delta;
   h.maxr2 = rtr;
-  h.ru_every = sloppy == Prec::F64 ? 0 : kRuEvery;
+  h.ru_every = sloppy == Prec::F64 ? 0 : (sloppy == Prec::F16 ? kRuEvery16 : kRuEvery);
   h.last_ru = 0;
   double best = rtr;  // smallest true |r|^2 so far
   int stall = 0;      // reliable updates in a row without progress
+  int forced = 0;     // periodic (not delta-triggered) reliable updates in a row
   bool stalled = false;
   int ru = 0;
   int nl = 5 + (sloppy != Prec::F64 ? 2 : 0);  // kernels launched so far
@@ -410,6 +415,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
       break;
     }
     // reliable update: x += x_s, r = b - A x in FP64
+    const bool periodic = !(h.rtr < h.delta2 * h.maxr2);
     nl += 7;
     launch_accum_x(g, x, (float4*)xs.v, c->stream);
     apply_mdagm(c, Prec::F64, S(ax), S(x), S(t64), S(q64), op);
@@ -426,6 +432,8 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     // stops falling (or grows) over several reliable updates
     if (rtrue < 0.5 * best) { best = rtrue; stall = 0; }
     else if (++stall >= 5 || rtrue > 1e4 * best) { h.rtr = rtrue; stalled = true; break; }
+    forced = periodic ? forced + 1 : 0;
+    if (sloppy == Prec::F16 && forced >= 2) { h.rtr = rtrue; stalled = true; break; }
     // continue from the true residual with p re-orthogonalised against it:
     // p = r + beta (p - (<r,p>/|r|^2) r), beta = |r|^2 / |r_old|^2
     launch_rdot(g, rs, sloppy, p, c->red, c->dres, c->stream);
