@@ -176,9 +176,9 @@ def build_system(bq, L, device, seed_skip, cool):
 
 # DRAM bytes (read + write) of one k_pass1<int16> launch per output site, from
 # one ncu capture at 32x32x32x32 (dram__bytes_read.sum + dram__bytes_write.sum
-# = 207.3 + 18.5 MB for 524288 sites); traffic grows with the number of
+# = 207.3 + 22.2 MB for 524288 sites); traffic grows with the number of
 # sites, so the per-launch figure at another volume is this times volh
-TRAFFIC_PER_SITE_INT16 = 430.6
+TRAFFIC_PER_SITE_INT16 = 437.6
 
 
 def stencil_bytes_per_site(prec):
