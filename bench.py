@@ -151,7 +151,11 @@ def allmax(pg, v, local):
     return float(t.item())
 
 
-def build_system(bq, L, device, seed_skip, cool):
+def lattice_of(args, default):
+    return tuple(int(x) for x in (args.lattice or default).split(","))
+
+
+def start_config(bq, L, device, cool):
     """Hot start, then conf_relax sweeps.  cool < 0: sweep until the plaquette
     (<Re Tr P>/3) first reaches PLAQ_TARGET, at most COOL sweeps."""
     lat = bq.Lattice(L, (1, 1, 1, -1), device=device)
@@ -166,6 +170,12 @@ def build_system(bq, L, device, seed_skip, cool):
             lat.conf_relax(1)
             sweeps += 1
     lat.sweeps = sweeps
+    return lat
+
+
+def build_system(bq, L, device, seed_skip, cool):
+    """start_config, the clover term, one Gaussian right-hand side."""
+    lat = start_config(bq, L, device, cool)
     lat.clover_init(CSW * KAPPA)
     lat.ranset(0, seed_skip)
     hb = lat.field()
@@ -199,7 +209,7 @@ def run_ours(args):
     import bqcdg as bq
 
     world, rank, local, pg = dist_init()
-    L = tuple(int(x) for x in args.lattice.split(","))
+    L = lattice_of(args, "32,32,32,64")
     peak, peak_kind = peaks()
     lat, hb, hx = build_system(bq, L, local, 1000003 * rank, args.cool)
     para = bq.HmcPara(kappa=KAPPA, csw=CSW)
@@ -349,7 +359,7 @@ def run_reference(args):
     if rank != 0:
         return
     from oracle import oracle as O
-    L = tuple(int(x) for x in args.lattice.split(","))
+    L = lattice_of(args, "32,32,32,64")
     g = O.Geom(L, (1, 1, 1, -1))
     O.ranset(0)
     u = g.hot()
@@ -420,7 +430,7 @@ def run_hmc(args):
     from bqcdg.hmc import Hmc, quenched_trajectory
 
     world, rank, local, pg = dist_init()
-    L = tuple(int(x) for x in (args.lattice if args.lattice != "32,32,32,64" else "24,24,24,48").split(","))
+    L = lattice_of(args, "24,24,24,48")
     kappa, kshift, beta = 0.1355, 0.13, 5.29
     lat, hb, _ = build_system(bq, L, local, 1000003 * rank, args.cool)
     therm = []
@@ -473,7 +483,7 @@ def run_batch(args):
     import bqcdg as bq
 
     world, rank, local, pg = dist_init()
-    L = tuple(int(x) for x in (args.lattice if args.lattice != "32,32,32,64" else "48,48,48,96").split(","))
+    L = lattice_of(args, "48,48,48,96")
     from bqcdg.hmc import quenched_trajectory
     kappa = 0.1355
     lat, hb, hx = build_system(bq, L, local, 1000003 * rank, args.cool)
@@ -547,18 +557,129 @@ def run_batch(args):
         pg.destroy_process_group()
 
 
+def run_shifts(args):
+    """Optional workload: 8 Gaussian right-hand sides at 64^3x128, each with
+    its own shift, in one batched mixed-precision CG.  The action is the
+    default one at kappa 0.136; the shifts are kappa_k from 0.134 to 0.136 in
+    BQCD's form W = M~ + rho_k, rho_k = 0.136/kappa_k - 1 (the Hasenbusch
+    relation of the hmc workload).  int16 links (12 reals) and spinors, FP64
+    reliable updates, stop at true |r|/|b| < 1e-10 per system; a converged
+    system retires inside the kernels while the others go on.  Then each
+    solution is compared with an FP64 CG solve of its own system (the FP64
+    operator is checked against the oracle by the test suite), and one
+    batched stencil launch is timed for the HBM roofline.  The gauge start is
+    the one of the batch workload; only the two clover parts the solver reads
+    are kept, and the thermalisation buffers are released before the solve,
+    so the 8 systems fit one GPU."""
+    import numpy as np
+    import bqcdg as bq
+    from bqcdg.hmc import quenched_trajectory
+
+    world, rank, local, pg = dist_init()
+    L = lattice_of(args, "64,64,64,128")
+    kappa, nrhs = 0.136, 8
+    kappas = np.linspace(0.134, 0.136, nrhs)
+    rhos = kappa / kappas - 1.0
+
+    t_start = time.perf_counter()
+
+    def mem(tag):
+        print("shifts: %6.1f s: %s, %.1f GB on the device" % (time.perf_counter() - t_start, tag,
+                                                               lat.device_bytes / 1e9), file=sys.stderr, flush=True)
+
+    lat = start_config(bq, L, local, args.cool)
+    therm = []
+    for _ in range(args.therm):
+        therm.append(round(quenched_trajectory(lat, 5.29, 1.0, 50, force_accept=True)[2], 5))
+    mem("after thermalisation")
+    lat.release_scratch(solver=True, hmc=True)
+    lat.clover_init_solver(CSW * kappa)
+    para = bq.HmcPara(kappa=kappa, csw=CSW)
+    lat.ranset(0, 1000003 * rank)
+    hbs = []
+    for _ in range(nrhs):
+        h = lat.field()
+        lat.field_gauss(h, 0.5)
+        hbs.append(h)
+    hxs = [lat.field() for _ in range(nrhs)]
+    mem("fields ready, plaquettes %s" % therm)
+    barrier(pg, local)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        infos = lat.solve_batch_shifted(hxs, hbs, para, rhos, precision=bq.PREC_HALF, tol=args.tol, block=nrhs)
+        wall = time.perf_counter() - t0
+    batch_s = allmax(pg, infos[0].seconds, local)
+    mem("after the batched solve")
+    # one batched first pass over the 8 solutions, and the single-RHS pass
+    ms_b = lat.time_pass_batch(hxs, para, bq.PREC_HALF, 20)
+    ms_1 = lat.time_pass(hxs[0], para, bq.PREC_HALF, 20)
+    volh = lat.volh
+    alg = volh * (8 * 24 + 148 + nrhs * 2 * 52)      # links and clover once, each spinor in and out
+    peak, peak_kind = peaks()
+    achieved = alg / (ms_b * 1e-3) / 1e9
+    # FP64 reference solve of each system, then the batched solution's error
+    lat.release_scratch(solver=True)
+    zero = np.zeros((volh, 3, 4), np.complex128)
+    errs, fp64 = [], []
+    for k in range(min(args.ref_rhs, nrhs)):
+        xb = lat.field_get(hxs[k])
+        lat.field_set(hxs[k], zero)
+        info = lat.solve_dev(hxs[k], hbs[k], para, precision=bq.PREC_DOUBLE, tol=args.tol, rho=float(rhos[k]))
+        xr = lat.field_get(hxs[k])
+        errs.append(float(np.linalg.norm(xb - xr) / np.linalg.norm(xr)))
+        fp64.append({"iterations": info.niter, "seconds": round(info.seconds, 3), "converged": info.converged})
+        print("shifts: rhs %d fp64 %d iterations %.2f s, rel error %.2e" % (k, info.niter, info.seconds, errs[-1]),
+              file=sys.stderr, flush=True)
+        del xb, xr
+    if rank == 0:
+        out = {"metric": "8-RHS shifted batched CG time-to-1e-10 at 64^3x128, kappa 0.136 (int16 iterations)",
+               "value": round(batch_s, 3), "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
+               "ms_per_step": round(1e3 * batch_s, 1), "higher_is_better": False, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64 (int16 sloppy iterations)",
+               "data": "synthetic: device hot start + %d conf_relax sweep(s) + %d forced-accept pure-gauge "
+                       "trajectories at beta 5.29 (plaquettes %s); 8 Gaussian right-hand sides"
+                       % (lat.sweeps, args.therm, therm),
+               "config": {"workload": "batched shifted M^+M CG, lattice %s, kappa %.4f, c_sw %.4f, 8 RHS with "
+                                      "kappa_k %s (rho_k = kappa/kappa_k - 1), one launch of 8"
+                                      % ("x".join(map(str, L)), kappa, CSW,
+                                         "-".join("%.4f" % x for x in kappas[[0, -1]])),
+                          "parallelism": "replicas x%d" % world},
+               "wall_s": round(wall, 3),
+               "rho": [round(float(r), 6) for r in rhos],
+               "iterations": [i.niter for i in infos],
+               "reliable_updates": [i.reliable_updates for i in infos],
+               "converged": all(i.converged for i in infos),
+               "true_rel_residual": [float("%.3e" % ((i.true_rtr / i.b2) ** 0.5)) for i in infos],
+               "fp64_rel_error": [float("%.3e" % e) for e in errs],
+               "fp64_reference": fp64,
+               "fp64_sequential_s": round(sum(f["seconds"] for f in fp64), 3),
+               "roofline": {"bound": "hbm", "kernel": "k_pass1<int16>, 8 right-hand sides per launch",
+                            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                            "frac": round(achieved / peak, 3), "peak_kind": peak_kind,
+                            "algorithmic_bytes_per_launch": alg, "ms_per_launch": round(ms_b, 4),
+                            "single_rhs_ms_per_launch": round(ms_1, 4)},
+               "clocks": clk.summary()}
+        print(json.dumps(out))
+    lat.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="solve", choices=["solve", "hmc", "batch"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "hmc", "batch", "shifts"],
                     help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories; "
-                         "batch: 16 right-hand sides")
+                         "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128")
     ap.add_argument("--therm", type=int, default=10,
-                    help="hmc, batch: forced-accept pure-gauge trajectories on the start configuration")
-    ap.add_argument("--lattice", default="32,32,32,64")
+                    help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
+    ap.add_argument("--ref-rhs", type=int, default=8, help="shifts: systems checked against an FP64 solve")
+    ap.add_argument("--lattice", default=None,
+                    help="x,y,z,t; default 32,32,32,64 (solve), 24,24,24,48 (hmc), 48,48,48,96 (batch), "
+                         "64,64,64,128 (shifts)")
     ap.add_argument("--cool", type=int, default=-1,
                     help="conf_relax sweeps; -1: until the plaquette reaches %.2f" % PLAQ_TARGET)
     ap.add_argument("--tol", type=float, default=1e-10)
@@ -575,6 +696,8 @@ def main():
         run_hmc(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "shifts":
+        run_shifts(args)
     else:
         run_ours(args)
 

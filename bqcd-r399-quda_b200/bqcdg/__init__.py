@@ -80,6 +80,8 @@ def _lib_handle():
         L.bqcdg_load_clover.argtypes = [vp, dp, dp, dp]
         L.bqcdg_get_clover.argtypes = [vp, dp, dp, dp]
         L.bqcdg_clover_init.argtypes = [vp, C.c_double]
+        L.bqcdg_clover_init_solver.argtypes = [vp, C.c_double]
+        L.bqcdg_release_scratch.argtypes = [vp, i]
         L.bqcdg_clover_action.argtypes = [vp, i, P(C.c_double)]
         for n in ("bqcdg_d", "bqcdg_d_dag"):
             getattr(L, n).argtypes = [vp, i, i, dp, dp]
@@ -104,8 +106,11 @@ def _lib_handle():
         L.bqcdg_solve_dev.argtypes = [vp, i, i, P(Params), P(SolverOpts), P(SolveInfo)]
         L.bqcdg_mdagm_dev.argtypes = [vp, i, i, P(Params), i, i, P(C.c_double)]
         L.bqcdg_time_pass.argtypes = [vp, i, P(Params), i, i, P(C.c_double)]
+        L.bqcdg_time_pass_batch.argtypes = [vp, i, P(C.c_int), P(Params), i, i, P(C.c_double)]
         L.bqcdg_solve_batch.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), P(SolverOpts), i,
                                         P(SolveInfo)]
+        L.bqcdg_solve_batch_shifted.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, P(SolverOpts), i,
+                                                P(SolveInfo)]
         L.bqcdg_ranset.argtypes = [vp, C.c_longlong, C.c_longlong]
         L.bqcdg_ranget.argtypes = [vp, P(C.c_longlong)]
         L.bqcdg_conf_hot.argtypes = [vp]
@@ -219,6 +224,17 @@ class Lattice:
     def clover_init(self, csw_kappa):
         """clover_init(a, i, b, u, csw_kappa) on the device from the loaded links."""
         _check(lib().bqcdg_clover_init(self.h, csw_kappa), "clover_init")
+
+    def release_scratch(self, solver=True, hmc=False):
+        """Free the device buffers that later calls re-create on demand:
+        the solver's work vectors and staging (solver), the resident momenta,
+        saved links and force buffers (hmc)."""
+        _check(lib().bqcdg_release_scratch(self.h, (1 if solver else 0) | (2 if hmc else 0)), "release_scratch")
+
+    def clover_init_solver(self, csw_kappa):
+        """clover_init keeping only the two parts the even-odd solver uses (A
+        even, A^-1 odd): a third of the clover memory of clover_init."""
+        _check(lib().bqcdg_clover_init_solver(self.h, csw_kappa), "clover_init_solver")
 
     def get_clover(self):
         out = [np.zeros((2, self.volh, 2, 18), np.complex128) for _ in range(3)]
@@ -494,6 +510,23 @@ class Lattice:
             _check(st, "solve_batch")
         return list(infos)
 
+    def solve_batch_shifted(self, hxs, hbs, para, rhos, precision=PREC_HALF, tol=1e-10, relative=True,
+                            maxiter=100000, delta=0.1, block=0):
+        """solve_batch with the shift rho of system k given by rhos[k]
+        (W = M~ + rho_k); the links and clover are shared."""
+        n = len(hxs)
+        if len(rhos) != n or len(hbs) != n:
+            raise ValueError("solve_batch_shifted: one b and one rho per x")
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0)
+        infos = (SolveInfo * n)()
+        prm = para.params(0.0) if isinstance(para, HmcPara) else para
+        r = np.ascontiguousarray(rhos, dtype=np.float64)
+        st = lib().bqcdg_solve_batch_shifted(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm),
+                                             r.ctypes.data, C.byref(o), block, infos)
+        if st not in (OK, ENOCONV):
+            _check(st, "solve_batch_shifted")
+        return list(infos)
+
     def mdagm_dev(self, hout, hin, para, precision, n, rho=None):
         ms = C.c_double()
         prm = para.params(rho) if isinstance(para, HmcPara) else para
@@ -504,4 +537,14 @@ class Lattice:
         ms = C.c_double()
         prm = para.params(rho) if isinstance(para, HmcPara) else para
         _check(lib().bqcdg_time_pass(self.h, hin, C.byref(prm), precision, n, C.byref(ms)), "time_pass")
+        return ms.value
+
+    def time_pass_batch(self, hins, para, precision, n, rho=None):
+        """Average device ms of one batched first stencil pass over the
+        resident fields hins (one launch serves all of them)."""
+        ms = C.c_double()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        k = len(hins)
+        _check(lib().bqcdg_time_pass_batch(self.h, k, (C.c_int * k)(*hins), C.byref(prm), precision, n,
+                                           C.byref(ms)), "time_pass_batch")
         return ms.value

@@ -37,8 +37,9 @@ struct bqcdg_ctx {
   Geom g{};
   long long bytes = 0;
   std::vector<void*> allocations;
+  std::vector<size_t> alloc_sizes;  // bytes of allocations[k]
 
-  double2* staging = nullptr;  // Fortran-layout staging (largest field: gauge)
+  double2* staging = nullptr;  // Fortran-layout staging, grown on demand (stage)
   size_t staging_bytes = 0;
 
   double2* gauge64 = nullptr;
@@ -64,6 +65,7 @@ struct bqcdg_ctx {
   RedScratch red{};
   double* dres = nullptr;        // device result scalars [16]
   double* hres = nullptr;        // pinned mirror
+  double* drho = nullptr;        // per right-hand-side shifts of a batch [kMaxRhs]
   CgScalars* dcg = nullptr;
   CgScalars* hcg = nullptr;      // pinned
 
@@ -72,7 +74,6 @@ struct bqcdg_ctx {
   double* mom_old = nullptr;     // their snapshot for the force monitor
   double2* gauge_bck = nullptr;  // saved links (restored on a rejected trajectory)
   double2* wbuf = nullptr;       // 6 planes x 9 complex per site
-  double2* tmpclov = nullptr;    // one parity of clover blocks
 
   std::map<int, double2*> fields;
   int next_handle = 1;
@@ -91,7 +92,9 @@ struct bqcdg_ctx {
     if (!p) return;
     for (size_t k = 0; k < allocations.size(); k++)
       if (allocations[k] == p) {
+        bytes -= (long long)alloc_sizes[k];
         allocations.erase(allocations.begin() + k);
+        alloc_sizes.erase(alloc_sizes.begin() + k);
         break;
       }
     cudaFree(p);
@@ -111,8 +114,20 @@ struct bqcdg_ctx {
     cudaError_t e = cudaMalloc(p, n);
     if (e == cudaSuccess) {
       allocations.push_back(*p);
+      alloc_sizes.push_back(n);
       bytes += (long long)n;
     }
+    return e;
+  }
+  // the staging buffer holds at least n bytes afterwards (a spinor needs
+  // 192 B per even site, a clover parity 576 B, the links 1152 B)
+  cudaError_t stage(size_t n) {
+    if (staging_bytes >= n) return cudaSuccess;
+    release(staging);
+    staging = nullptr;
+    staging_bytes = 0;
+    cudaError_t e = alloc((void**)&staging, n);
+    if (e == cudaSuccess) staging_bytes = n;
     return e;
   }
   double2* sp64(size_t k) {
@@ -167,6 +182,7 @@ CloverPtr C(double2* p) {
 
 int upload_spinor(bqcdg_ctx* c, const double* host, double2* dev) {
   size_t n = (size_t)c->g.volh * 12 * sizeof(double2);
+  CK(c->stage(n));
   CK(cudaMemcpyAsync(c->staging, host, n, cudaMemcpyHostToDevice, c->stream));
   launch_spinor_from_fortran(c->g, dev, c->staging, c->stream);
   CKL();
@@ -175,6 +191,7 @@ int upload_spinor(bqcdg_ctx* c, const double* host, double2* dev) {
 
 int download_spinor(bqcdg_ctx* c, const double2* dev, double* host) {
   size_t n = (size_t)c->g.volh * 12 * sizeof(double2);
+  CK(c->stage(n));
   launch_spinor_to_fortran(c->g, c->staging, dev, c->stream);
   CKL();
   CK(cudaMemcpyAsync(host, c->staging, n, cudaMemcpyDeviceToHost, c->stream));
@@ -565,18 +582,28 @@ int fp64_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Spin
 // side has its own scalars, stops and FP64 reliable updates, and a converged
 // or paused one costs its CTAs an early return only.
 int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op, Prec sloppy, int maxiter,
-             const double* stop, double delta, bqcdg_solve_info* info) {
+             const double* stop, double delta, bqcdg_solve_info* info, const double* rho = nullptr) {
   const Geom& g = c->g;
   int st = ensure_sloppy(c, sloppy, op.csw_kappa != 0.0);
   if (st) return st;
   if ((st = ensure_batch(c, sloppy, nb))) return st;
   auto& B = c->batch;
+  // the operator of right-hand side k: op, with its own shift when rho is given
+  std::vector<OpParams> ops(nb, op);
+  const double* drho = nullptr;
+  if (rho) {
+    for (int k = 0; k < nb; k++) ops[k].rho = rho[k];
+    std::memcpy(c->hres, rho, sizeof(double) * nb);
+    CK(cudaMemcpyAsync(c->drho, c->hres, sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));  // hres is reused below
+    drho = c->drho;
+  }
   CK(cudaEventRecord(c->ev0, c->stream));
   std::vector<int> ru(nb, 0), fin(nb, 0), conv(nb, 0), nl(nb, 0), stall(nb, 0), stalled(nb, 0);
   std::vector<double> best(nb, 0.0);
   for (int k = 0; k < nb; k++) {
     double r2, b2;
-    if ((st = fp64_residual(c, x[k], b[k], op, rhs_of(B.rs, k), &r2, &b2))) return st;
+    if ((st = fp64_residual(c, x[k], b[k], ops[k], rhs_of(B.rs, k), &r2, &b2))) return st;
     launch_spinor_convert(g, sloppy, rhs_of(B.p, k), Prec::F32, rhs_of(B.rs, k), c->stream);
     launch_zero(g, Prec::F32, rhs_of(B.xs, k), c->stream);
     CKL();
@@ -607,11 +634,11 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
       launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
                         nb);
       launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
-                        c->dcg, c->stream, nb);
+                        c->dcg, c->stream, nb, drho);
       launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
                         nb);
       launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
-                      c->dcg, c->stream, nb);
+                      c->dcg, c->stream, nb, true, drho);
       launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
     }
     launches += 5 * batch;
@@ -627,7 +654,7 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
       // reliable update of right-hand side k: x += x_s, r = b - A x in FP64
       launch_accum_x(g, x[k], (float4*)rhs_of(B.xs, k).v, c->stream);
       double rt;
-      if ((st = fp64_residual(c, x[k], b[k], op, rhs_of(B.rs, k), &rt, nullptr))) return st;
+      if ((st = fp64_residual(c, x[k], b[k], ops[k], rhs_of(B.rs, k), &rt, nullptr))) return st;
       ru[k]++;
       launches += 7;
       if (!(rt == rt)) { h.done = 4; fin[k] = 1; continue; }
@@ -683,7 +710,7 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
     if (!stalled[k]) continue;
     bqcdg_solve_info more;
     std::memset(&more, 0, sizeof(more));
-    int st2 = cg_robust(c, x[k], b[k], op, sloppy == Prec::F16 ? Prec::F32 : Prec::F64,
+    int st2 = cg_robust(c, x[k], b[k], ops[k], sloppy == Prec::F16 ? Prec::F32 : Prec::F64,
                         maxiter - info[k].niter, stop[k], delta, false, false, &more);
     if (st2) return st2;
     info[k].niter += more.niter;
@@ -781,14 +808,13 @@ int bqcdg_create(bqcdg_ctx** out, const int L[4], const int bc[4], int device) {
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
-  c->staging_bytes = (size_t)c->g.volh * 72 * sizeof(double2);
-  if (e == cudaSuccess) e = c->alloc((void**)&c->staging, c->staging_bytes);
   c->red.maxblocks = nblocks(c->g.volh);
   if (e == cudaSuccess)
     e = c->alloc((void**)&c->red.partial, sizeof(double) * kRedVals * kMaxRhs * c->red.maxblocks);
   if (e == cudaSuccess) e = c->alloc((void**)&c->red.counter, sizeof(unsigned int) * kMaxRhs);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->red.counter, 0, sizeof(unsigned int) * kMaxRhs, c->stream);
   if (e == cudaSuccess) e = c->alloc((void**)&c->dres, sizeof(double) * 16);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->drho, sizeof(double) * kMaxRhs);
   if (e == cudaSuccess) e = c->alloc((void**)&c->dcg, sizeof(CgScalars) * kMaxRhs);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hres, sizeof(double) * 16);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hcg, sizeof(CgScalars) * kMaxRhs);
@@ -818,11 +844,50 @@ int bqcdg_destroy(bqcdg_ctx* c) {
 int bqcdg_volh(const bqcdg_ctx* c) { return c ? c->g.volh : -1; }
 long long bqcdg_device_bytes(const bqcdg_ctx* c) { return c ? c->bytes : -1; }
 
+int bqcdg_release_scratch(bqcdg_ctx* c, int what) {
+  if (!c || what < 0 || what > (BQCDG_SCRATCH_SOLVER | BQCDG_SCRATCH_HMC)) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  if (what & BQCDG_SCRATCH_SOLVER) {
+    c->release(c->staging);
+    c->staging = nullptr;
+    c->staging_bytes = 0;
+    for (double2* p : c->s64) c->release(p);
+    c->s64.clear();
+    for (std::vector<SpinorPtr>* pool : {&c->s32, &c->s16}) {
+      for (SpinorPtr& sp : *pool) {
+        c->release(sp.v);
+        c->release(sp.norm);
+      }
+      pool->clear();
+    }
+    auto& B = c->batch;
+    for (SpinorPtr* sp : {&B.p, &B.t, &B.q, &B.rs, &B.xs}) {
+      c->release(sp->v);
+      c->release(sp->norm);
+      *sp = SpinorPtr{};
+    }
+    B.cap = 0;
+  }
+  if (what & BQCDG_SCRATCH_HMC) {
+    for (double** p : {&c->pgen, &c->mom, &c->mom_old}) {
+      c->release(*p);
+      *p = nullptr;
+    }
+    for (double2** p : {&c->wbuf, &c->gauge_bck}) {
+      c->release(*p);
+      *p = nullptr;
+    }
+  }
+  return BQCDG_OK;
+}
+
 int bqcdg_load_gauge(bqcdg_ctx* c, const double* u, int flipped) {
   if (!c || !u) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
   size_t n = (size_t)c->g.volh * 72 * sizeof(double2);
+  CK(c->stage(n));
   CK(cudaMemcpyAsync(c->staging, u, n, cudaMemcpyHostToDevice, c->stream));
   launch_gauge_from_fortran(c->g, c->gauge64, c->staging, flipped, c->stream);
   CKL();
@@ -841,6 +906,7 @@ int bqcdg_get_gauge(bqcdg_ctx* c, double* u, int flipped) {
   if (!c || !u) return BQCDG_EINVAL;
   if (!c->have_gauge) return BQCDG_ENOGAUGE;
   CK(cudaSetDevice(c->device));
+  CK(c->stage((size_t)c->g.volh * 72 * sizeof(double2)));
   launch_gauge_to_fortran(c->g, c->staging, c->gauge64, flipped, c->stream);
   CKL();
   CK(cudaMemcpyAsync(u, c->staging, (size_t)c->g.volh * 72 * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
@@ -852,6 +918,7 @@ static int load_clover_field(bqcdg_ctx* c, double2** dst, bool* have, const doub
   for (int eo = 0; eo < 2; eo++) {
     if (!dst[eo]) CK(c->alloc((void**)&dst[eo], (size_t)36 * c->g.stride * sizeof(double2)));
     size_t n = (size_t)c->g.volh * 36 * sizeof(double2);
+    CK(c->stage(n));
     CK(cudaMemcpyAsync(c->staging, src + (size_t)eo * c->g.volh * 72, n, cudaMemcpyHostToDevice, c->stream));
     launch_clover_from_fortran(c->g, dst[eo], c->staging, c->stream);
     CKL();
@@ -884,6 +951,7 @@ int bqcdg_load_clover(bqcdg_ctx* c, const double* a, const double* ainv, const d
 static int get_clover_field(bqcdg_ctx* c, double2** srcs, const bool* have, double* dst) {
   for (int eo = 0; eo < 2; eo++) {
     if (!have[eo]) return BQCDG_ENOCLOVER;
+    CK(c->stage((size_t)c->g.volh * 36 * sizeof(double2)));
     launch_clover_to_fortran(c->g, c->staging, srcs[eo], c->stream);
     CKL();
     CK(cudaMemcpyAsync(dst + (size_t)eo * c->g.volh * 72, c->staging, (size_t)c->g.volh * 36 * sizeof(double2),
@@ -917,6 +985,32 @@ int bqcdg_clover_init(bqcdg_ctx* c, double csw_kappa) {
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   for (int eo = 0; eo < 2; eo++) c->have_A[eo] = c->have_Ainv[eo] = c->have_B[eo] = true;
+  for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  return BQCDG_OK;
+}
+
+int bqcdg_clover_init_solver(bqcdg_ctx* c, double csw_kappa) {
+  if (!c) return BQCDG_EINVAL;
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  // only A_ee and A_oo^-1; the other four fields are released if present
+  double2** unused[4] = {&c->A[1], &c->Ainv[0], &c->B[0], &c->B[1]};
+  for (double2** f : unused) {
+    c->release(*f);
+    *f = nullptr;
+  }
+  const size_t n = (size_t)36 * c->g.stride * sizeof(double2);
+  if (!c->A[0]) CK(c->alloc((void**)&c->A[0], n));
+  if (!c->Ainv[1]) CK(c->alloc((void**)&c->Ainv[1], n));
+  double2* a[2] = {c->A[0], nullptr};
+  double2* ai[2] = {nullptr, c->Ainv[1]};
+  double2* b[2] = {nullptr, nullptr};
+  launch_clover_init(c->g, c->gauge64, csw_kappa, a, ai, b, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_A[0] = c->have_Ainv[1] = true;
+  c->have_A[1] = c->have_Ainv[0] = c->have_B[0] = c->have_B[1] = false;
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
   return BQCDG_OK;
 }
@@ -1280,6 +1374,7 @@ int bqcdg_field_destroy(bqcdg_ctx* c, int h) {
 int bqcdg_field_gauss(bqcdg_ctx* c, int h, double var) {
   if (!c || !field(c, h)) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
+  CK(c->stage((size_t)c->g.volh * 12 * sizeof(double2)));
   launch_ran_gauss(c->staging, c->g.volh, 12, var, c->seed, c->stream);
   c->seed = ranf_skip(c->seed, 2ull * 12ull * (unsigned long long)c->g.volh);
   launch_spinor_from_fortran(c->g, field(c, h), c->staging, c->stream);
@@ -1323,6 +1418,7 @@ int bqcdg_conf_hot(bqcdg_ctx* c) {
   if (!c) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
+  CK(c->stage((size_t)c->g.volh * 72 * sizeof(double2)));
   const unsigned long long per = 2ull * 9ull * (unsigned long long)c->g.volh;
   for (int me = 0; me < 8; me++) {  // do mu; do eo (conf.F90:208-214)
     launch_ran_gauss(c->staging + (size_t)me * c->g.volh * 9, c->g.volh, 9, 1.0, c->seed, c->stream);
@@ -1337,6 +1433,7 @@ int bqcdg_conf_cold(bqcdg_ctx* c) {
   if (!c) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * c->g.stride * sizeof(double2)));
+  CK(c->stage((size_t)c->g.volh * 72 * sizeof(double2)));
   launch_cold(c->staging, 8LL * c->g.volh, c->stream);
   CKL();
   return gauge_finish(c);
@@ -1375,11 +1472,15 @@ int bqcdg_solve_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const b
   return solve_resident(c, field(c, hx), field(c, hb), p, o, info);
 }
 
-int bqcdg_solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
-                      const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+// rho: one shift per right-hand side (null: p->rho for all)
+static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
+                       const double* rho, const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
   int st = check_op(c, p);
   if (st) return st;
   if (!o || !hx || !hb || !infos || nrhs <= 0 || block < 0 || block > kMaxRhs) return BQCDG_EINVAL;
+  if (rho)
+    for (int k = 0; k < nrhs; k++)
+      if (!(rho[k] == rho[k])) return BQCDG_EINVAL;
   for (int k = 0; k < nrhs; k++)
     if (!field(c, hx[k]) || !field(c, hb[k])) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
@@ -1412,18 +1513,32 @@ int bqcdg_solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, cons
       xs[k] = field(c, hx[k0 + k]);
       bs[k] = field(c, hb[k0 + k]);
     }
-    st = cg_batch(c, xs.data(), bs.data(), nb, op, sl, o->maxiter, stop.data() + k0, o->delta, infos + k0);
+    st = cg_batch(c, xs.data(), bs.data(), nb, op, sl, o->maxiter, stop.data() + k0, o->delta, infos + k0,
+                  rho ? rho + k0 : nullptr);
     if (st) return st;
     for (int k = 0; k < nb; k++) {
       bqcdg_solve_info& in = infos[k0 + k];
       if (o->check_true_residual) {
-        if ((st = true_residual(c, xs[k], bs[k], op, &in.true_rtr))) return st;
+        OpParams opk = op;
+        if (rho) opk.rho = rho[k0 + k];
+        if ((st = true_residual(c, xs[k], bs[k], opk, &in.true_rtr))) return st;
         in.converged = in.true_rtr <= stop[k0 + k] ? 1 : 0;
       }
       all_conv = all_conv && in.converged;
     }
   }
   return all_conv ? BQCDG_OK : BQCDG_ENOCONV;
+}
+
+int bqcdg_solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
+                      const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+  return solve_batch(c, nrhs, hx, hb, p, nullptr, o, block, infos);
+}
+
+int bqcdg_solve_batch_shifted(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
+                              const double* rho, const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+  if (!rho) return BQCDG_EINVAL;
+  return solve_batch(c, nrhs, hx, hb, p, rho, o, block, infos);
 }
 
 int bqcdg_mdagm_dev(bqcdg_ctx* c, int hout, int hin, const bqcdg_params* p, int precision, int n, double* ms) {
@@ -1479,6 +1594,34 @@ int bqcdg_time_pass(bqcdg_ctx* c, int hin, const bqcdg_params* p, int precision,
   CK(cudaEventRecord(c->ev0, c->stream));
   for (int k = 0; k < n; k++)
     launch_mtil_pass1(pr, geom_of(c, pr), false, t, in, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream);
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  float t_ms = 0.f;
+  cudaEventElapsedTime(&t_ms, c->ev0, c->ev1);
+  if (ms) *ms = t_ms / n;
+  return BQCDG_OK;
+}
+
+int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_params* p, int precision, int n,
+                          double* ms) {
+  int st = check_op(c, p);
+  if (st) return st;
+  if (!hin || nrhs <= 0 || nrhs > kMaxRhs || n <= 0) return BQCDG_EINVAL;
+  for (int k = 0; k < nrhs; k++)
+    if (!field(c, hin[k])) return BQCDG_EINVAL;
+  Prec pr = prec_of(precision);
+  if (pr == Prec::F64) return BQCDG_EUNSUPPORTED;  // batches are sloppy-precision
+  CK(cudaSetDevice(c->device));
+  OpParams op = op_of(p, true);
+  if ((st = ensure_sloppy(c, pr, p->csw_kappa != 0.0))) return st;
+  if ((st = ensure_batch(c, pr, nrhs))) return st;
+  auto& B = c->batch;
+  for (int k = 0; k < nrhs; k++) launch_spinor_convert(c->g, pr, rhs_of(B.p, k), Prec::F64, S(field(c, hin[k])), c->stream);
+  CKL();
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int k = 0; k < n; k++)
+    launch_mtil_pass1(pr, c->g, false, B.t, B.p, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream, nrhs);
   CK(cudaEventRecord(c->ev1, c->stream));
   CKL();
   CK(cudaStreamSynchronize(c->stream));

@@ -104,8 +104,11 @@ __device__ __forceinline__ void store_packed(double2* dst, int stride, int i, in
 }
 
 // clover_inv (clover_inv.F90:29-220) on an unhalved block a; writes the
-// halved A, the halved inverse and the B factors (L, halved 1/D)
+// halved A, the halved inverse and the B factors (L, halved 1/D), each only
+// when its destination is given
 __device__ void block_inv(const Blk& a, double2* A, double2* Ainv, double2* B, int stride, int i, int chi) {
+  if (A) store_packed(A, stride, i, chi, a, 0.5);
+  if (!Ainv && !B) return;
   C64 L[6][6];
   double d[6], dinv[6];
   for (int r = 0; r < 6; r++) {
@@ -122,12 +125,15 @@ __device__ void block_inv(const Blk& a, double2* A, double2* Ainv, double2* B, i
     dinv[r] = 1.0 / dr;
   }
   // B = (L, 1/D / 2)
-  double2* bb = B + chi * 18 * stride + i;
-  for (int r = 1; r < 6; r++)
-    for (int c = 0; c < r; c++) bb[(r * (r - 1) / 2 + c) * stride] = make_double2(L[r][c].x, L[r][c].y);
-  bb[15 * stride] = make_double2(0.5 * dinv[0], 0.5 * dinv[1]);
-  bb[16 * stride] = make_double2(0.5 * dinv[2], 0.5 * dinv[3]);
-  bb[17 * stride] = make_double2(0.5 * dinv[4], 0.5 * dinv[5]);
+  if (B) {
+    double2* bb = B + chi * 18 * stride + i;
+    for (int r = 1; r < 6; r++)
+      for (int c = 0; c < r; c++) bb[(r * (r - 1) / 2 + c) * stride] = make_double2(L[r][c].x, L[r][c].y);
+    bb[15 * stride] = make_double2(0.5 * dinv[0], 0.5 * dinv[1]);
+    bb[16 * stride] = make_double2(0.5 * dinv[2], 0.5 * dinv[3]);
+    bb[17 * stride] = make_double2(0.5 * dinv[4], 0.5 * dinv[5]);
+  }
+  if (!Ainv) return;
   // clover_inv2: columns of A^-1 by unit solves, stored halved (upper part)
   Blk inv;
   for (int col = 0; col < 6; col++) {
@@ -148,7 +154,6 @@ __device__ void block_inv(const Blk& a, double2* A, double2* Ainv, double2* B, i
     for (int k = col + 1; k < 6; k++) inv.m[col][k] = conjg(x[k]);
   }
   store_packed(Ainv, stride, i, chi, inv, 0.5);
-  store_packed(A, stride, i, chi, a, 0.5);
 }
 
 __global__ void __launch_bounds__(64) k_clover_init(Geom g, const double2* gauge, double factor, double2* a0,
@@ -157,6 +162,7 @@ __global__ void __launch_bounds__(64) k_clover_init(Geom g, const double2* gauge
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int eo = blockIdx.y;
   if (i >= g.volh) return;
+  if (!(eo == 0 ? (a0 || ai0 || b0) : (a1 || ai1 || b1))) return;  // nothing wanted of this parity
   Site st = site_coords(g, i, eo);
   Blk p, q;
   L64 f, f2;

@@ -282,10 +282,11 @@ template <Prec P, bool DAG, bool REDUCE>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
                                                   const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                                                   double hval, double rho, RedScratch red, double* norm_out,
-                                                  CgScalars* cg, int nr) {
+                                                  CgScalars* cg, int nr, const double* rho_rhs) {
   using R = typename SpinorView<P>::R;
   const Tile tl = tile(nr);
   if (cg && cg[tl.rhs].done) return;  // retired right-hand side
+  if (rho_rhs) rho = rho_rhs[tl.rhs];   // a shift per right-hand side
   const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
 
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s, int nr) {
+                       CgScalars* cg, cudaStream_t s, int nr, const double* rho_rhs) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
@@ -332,7 +333,7 @@ void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorP
   bool reduce = norm_out != nullptr || cg != nullptr;
 #define P2(PP, D, RR)                                                                                                \
   k_pass2<PP, D, RR><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, norm_out, \
-                                             cg, nr)
+                                             cg, nr, rho_rhs)
 #define P2R(PP, D) \
   if (reduce) P2(PP, D, true); else P2(PP, D, false);
   if (p == Prec::F64) { if (dag) { P2R(Prec::F64, true) } else { P2R(Prec::F64, false) } }
@@ -360,12 +361,13 @@ template <Prec P, Prec XP, bool XUPD>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
-                                                     RedScratch red, CgScalars* cgs, int nr) {
+                                                     RedScratch red, CgScalars* cgs, int nr, const double* rho_rhs) {
   using R = typename SpinorView<P>::R;
   using RX = typename SpinorView<XP>::R;
   const Tile tl = tile(nr);
   CgScalars* cg = cgs + tl.rhs;
   if (cg->done) return;  // retired right-hand side
+  if (rho_rhs) rho = rho_rhs[tl.rhs];  // a shift per right-hand side
   const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
@@ -429,14 +431,14 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
 
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr, bool xupd) {
+                     cudaStream_t s, int nr, bool xupd, const double* rho_rhs) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = -op.h;  // mtil_dag
 #define P4(PP, XX, XU)                                                                                          \
   k_cg_pass4<PP, XX, XU><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec, x, r, red, \
-                                                 cg, nr)
+                                                 cg, nr, rho_rhs)
   if (p == Prec::F64) { if (xupd) P4(Prec::F64, Prec::F64, true); else P4(Prec::F64, Prec::F64, false); }
   else if (p == Prec::F32) { if (xupd) P4(Prec::F32, Prec::F32, true); else P4(Prec::F32, Prec::F32, false); }
   else { if (xupd) P4(Prec::F16, Prec::F32, true); else P4(Prec::F16, Prec::F32, false); }

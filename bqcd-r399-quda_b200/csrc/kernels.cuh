@@ -81,13 +81,15 @@ void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorP
 // optional |out|^2 reduction into *norm_out (device), and CG alpha update
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s, int nr = 1);
+                       CgScalars* cg, cudaStream_t s, int nr = 1, const double* rho_rhs = nullptr);
 // CG-fused second half of mtil_dag: Ap = A_ee q + b D_eo t_o + rho q computed in
 // registers; x += alpha p, r -= alpha Ap, rtr = |r|^2.  Precision P for the
 // stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr = 1, bool xupd = true);
+                     cudaStream_t s, int nr = 1, bool xupd = true, const double* rho_rhs = nullptr);
+// (rho_rhs: device array of one shift rho per right-hand side, replacing
+//  op.rho, in the second passes; null: op.rho for all)
 // p = r + beta p; with x given (xupd = false above, single RHS), also the
 // x += alpha p of iteration `expect` if that iteration ran
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,

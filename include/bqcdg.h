@@ -103,6 +103,16 @@ const char *bqcdg_error_string(int status);
 int bqcdg_volh(const bqcdg_ctx *ctx);
 /* device memory held by the context, bytes */
 long long bqcdg_device_bytes(const bqcdg_ctx *ctx);
+/* free device memory that later calls re-create on demand, for lattices that
+ * fill the GPU.  BQCDG_SCRATCH_SOLVER: the solver's work vectors, the batch
+ * buffers and the Fortran-layout staging buffer.  BQCDG_SCRATCH_HMC: the
+ * resident momenta (until bqcdg_mom_gauss or bqcdg_mom_set makes new ones
+ * the momentum entry points return BQCDG_EINVAL), the saved links of
+ * bqcdg_gauge_save and the force work buffers.  Links, clover, the sloppy
+ * copies of both and the resident fields are kept. */
+#define BQCDG_SCRATCH_SOLVER 1
+#define BQCDG_SCRATCH_HMC 2
+int bqcdg_release_scratch(bqcdg_ctx *ctx, int what);
 
 /* ---- fields ----------------------------------------------------------- */
 /* conf%u; flipped = 1 if flip_bc() has been applied to the array.
@@ -116,6 +126,12 @@ int bqcdg_get_clover(bqcdg_ctx *ctx, double *a, double *ainv, double *b);
 /* clover_init(a, i, b, u, csw_kappa) (clover/clover_init.F90:28) on the
  * device, from the loaded links */
 int bqcdg_clover_init(bqcdg_ctx *ctx, double csw_kappa);
+/* clover_init for the even-odd solver only: A of the even sites and A^-1 of
+ * the odd sites (clover_init.F90:28 + clover_inv.F90:29), the two fields that
+ * M~ and W use; the other four (A odd, A^-1 even, the B factors) are released.
+ * A third of the memory of bqcdg_clover_init, for lattices where all six do
+ * not fit; entry points that need the others then return BQCDG_ENOCLOVER. */
+int bqcdg_clover_init_solver(bqcdg_ctx *ctx, double csw_kappa);
 /* clover_action(b(1,1,ODD)) (clover/clover_action.F90:29) */
 int bqcdg_clover_action(bqcdg_ctx *ctx, int eo, double *action);
 
@@ -202,12 +218,23 @@ int bqcdg_solve_dev(bqcdg_ctx *ctx, int hx, int hb, const bqcdg_params *p, const
  * launch (1..16; 0 = choose by timing 1, 4, 8 and 16).  infos: nrhs entries. */
 int bqcdg_solve_batch(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
                       const bqcdg_solver_opts *o, int block, bqcdg_solve_info *infos);
+/* bqcdg_solve_batch with a shift per right-hand side: system k is
+ * (W^+W) x_k = b_k with W = M~ + rho[k] (m_tilde.F90:63-73), the links and
+ * clover shared.  These are the solves of the pseudofermion levels of
+ * mass-preconditioned HMC, which differ only in rho (dsf1.F90:66 with
+ * para%rho, dsf2.F90:64 with rho = 0); p->rho is ignored. */
+int bqcdg_solve_batch_shifted(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
+                              const double *rho, const bqcdg_solver_opts *o, int block, bqcdg_solve_info *infos);
 /* out = (W^+W) in with both resident, repeated n times; *ms = average device
  * time of one application (CUDA events on the context stream) */
 int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);
 /* average device time of one even-odd stencil pass (pass 1 of mtil: D_oe,
  * Ainv_oo) at the given precision, n launches */
 int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precision, int n, double *ms);
+/* the same for the batched pass over nrhs right-hand sides hin[0..nrhs-1]
+ * (1..16; FP32 or int16): average device time of one launch serving all */
+int bqcdg_time_pass_batch(bqcdg_ctx *ctx, int nrhs, const int *hin, const bqcdg_params *p, int precision, int n,
+                          double *ms);
 
 /* ---- resident HMC pieces ------------------------------------------------ */
 /* With these a trajectory keeps the links, the momenta and its spinor fields

@@ -55,3 +55,124 @@ def test_batch_retires_converged_rhs(setup, bq):
     infos = lat.solve_batch(hx, [h0, h1], para, tol=1e-10, relative=False, block=2)
     assert infos[0].niter == 0 and infos[0].converged == 1, infos[0].as_dict()
     assert infos[1].converged == 1 and infos[1].niter > 0, infos[1].as_dict()
+
+
+@pytest.fixture(scope="module")
+def oracle_setup(oracle, bq):
+    L = (8, 8, 8, 8)
+    g = oracle.Geom(L, (1, 1, 1, -1))
+    oracle.ranset(2468)
+    u = g.hot()
+    uf = g.flip_bc(u.copy())
+    kappa, csw = 0.13, 1.9192
+    clov = g.clover_init(u, csw * kappa)
+    lat = bq.Lattice(L, (1, 1, 1, -1))
+    lat.load_gauge(uf, flipped=True)
+    lat.load_clover(*clov)
+    yield dict(g=g, uf=uf, clov=clov, lat=lat, kappa=kappa, csw=csw)
+    lat.close()
+
+
+@pytest.mark.parametrize("block", [3, 0])
+def test_shifted_batch_matches_oracle_cg(oracle_setup, bq, block):
+    """System k is (W^+W) x = b with W = M~ + rho_k (m_tilde.F90:63-73): each
+    solution equals the oracle's FP64 CG of w_dagger_w at that rho, one
+    right-hand side appears twice with different shifts, and rho = 0 gives
+    the mtdagmt system of dsf2.F90:64."""
+    s = oracle_setup
+    g, lat = s["g"], s["lat"]
+    para = bq.HmcPara(kappa=s["kappa"], csw=s["csw"])
+    rhos = [0.0, 0.05, 0.3, 0.05, 1.0]
+    bs = [g.gauss_spinor(0) for _ in range(4)]
+    bs.append(bs[1].copy())                  # the same b as system 1, another rho
+    rhos[4] = 0.3
+    hb = [lat.field(b) for b in bs]
+    zero = np.zeros_like(bs[0])
+    hx = [lat.field(zero) for _ in bs]
+    infos = lat.solve_batch_shifted(hx, hb, para, rhos, tol=1e-10, block=block)
+    xs = []
+    for k, (b, rho) in enumerate(zip(bs, rhos)):
+        assert infos[k].converged == 1, infos[k].as_dict()
+        assert infos[k].true_rtr <= 1e-20 * infos[k].b2
+        name = "w_dagger_w" if rho else "mtdagmt"
+        xr, _, _, rc = g.cg(name, zero, b, s["uf"], s["clov"], s["kappa"], s["csw"] * s["kappa"], 0.0, rho,
+                            rest=1e-22 * float(np.vdot(b, b).real), maxiter=5000, log=0)
+        assert rc == 0
+        x = lat.field_get(hx[k])
+        assert np.linalg.norm(x - xr) <= 1e-8 * np.linalg.norm(xr), (k, rho)
+        xs.append(x)
+    # the shift is applied per system: same b, rho 0.05 vs 0.3
+    assert np.linalg.norm(xs[1] - xs[4]) > 1e-3 * np.linalg.norm(xs[1])
+
+
+def test_shifted_batch_rejects_missing_rho(oracle_setup, bq):
+    lat = oracle_setup["lat"]
+    para = bq.HmcPara(kappa=0.13, csw=1.9192)
+    h = lat.field()
+    with pytest.raises(ValueError):
+        lat.solve_batch_shifted([h], [h], para, [0.1, 0.2])
+
+
+def test_solver_only_clover_gives_the_same_solution(bq):
+    """clover_init_solver keeps A (even) and A^-1 (odd) only: the solver's
+    result is unchanged, the context holds less memory, and the entry points
+    that need the released parts say so."""
+    L = (8, 8, 8, 8)
+    para = bq.HmcPara(kappa=0.13, csw=1.9192, rho=0.1)
+    out = []
+    for solver_only in (False, True):
+        lat = bq.Lattice(L, (1, 1, 1, -1))
+        lat.ranset(5)
+        lat.conf_hot()
+        lat.conf_relax(1)
+        if solver_only:
+            lat.clover_init_solver(para.csw_kappa)
+        else:
+            lat.clover_init(para.csw_kappa)
+        lat.ranset(77)
+        hb = lat.field()
+        lat.field_gauss(hb, 0.5)
+        hx = lat.field(np.zeros((lat.volh, 3, 4), np.complex128))
+        info = lat.solve_dev(hx, hb, para, precision=bq.PREC_DOUBLE, tol=1e-12)
+        assert info.converged == 1
+        out.append((lat.field_get(hx), lat.device_bytes))
+        if solver_only:
+            with pytest.raises(bq.BqcdgError) as e:
+                lat.clover_action(1)
+            assert e.value.status == bq.ENOCLOVER
+        lat.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[1][1] < out[0][1]
+
+
+def test_release_scratch_frees_and_recreates(bq):
+    """release_scratch gives back the work buffers; the next solve re-creates
+    them and returns the same solution, and released momenta must be made
+    again before the momentum entry points accept a call."""
+    L = (8, 8, 8, 8)
+    para = bq.HmcPara(kappa=0.13, csw=1.9192, rho=0.1)
+    lat = bq.Lattice(L, (1, 1, 1, -1))
+    lat.ranset(3)
+    lat.conf_hot()
+    lat.clover_init(para.csw_kappa)
+    lat.ranset(4)
+    hb = lat.field()
+    lat.field_gauss(hb, 0.5)
+    zero = np.zeros((lat.volh, 3, 4), np.complex128)
+    hx = lat.field(zero)
+    lat.solve_batch([hx], [hb], para, tol=1e-10, block=1)
+    x1 = lat.field_get(hx)
+    lat.mom_gauss()
+    before = lat.device_bytes
+    lat.release_scratch(solver=True, hmc=True)
+    after = lat.device_bytes
+    assert after < before
+    with pytest.raises(bq.BqcdgError) as e:
+        lat.mom_action()
+    assert e.value.status == bq.EINVAL
+    lat.field_set(hx, zero)
+    lat.solve_batch([hx], [hb], para, tol=1e-10, block=1)
+    assert np.array_equal(lat.field_get(hx), x1)
+    lat.mom_gauss()
+    assert lat.mom_action() > 0
+    lat.close()
