@@ -613,6 +613,7 @@ def run_shifts(args):
     # one batched first pass over the 8 solutions, and the single-RHS pass
     ms_b = lat.time_pass_batch(hxs, para, bq.PREC_HALF, 20)
     ms_1 = lat.time_pass(hxs[0], para, bq.PREC_HALF, 20)
+    ms_nbt = {k: round(lat.time_pass_batch(hxs, para, bq.PREC_HALF, 20, rhs_per_thread=k), 4) for k in (1, 2, 4)}
     volh = lat.volh
     alg = volh * (8 * 24 + 148 + nrhs * 2 * 52)      # links and clover once, each spinor in and out
     peak, peak_kind = peaks()
@@ -640,7 +641,8 @@ def run_shifts(args):
                        "trajectories at beta 5.29 (plaquettes %s); 8 Gaussian right-hand sides"
                        % (lat.sweeps, args.therm, therm),
                "config": {"workload": "batched shifted M^+M CG, lattice %s, kappa %.4f, c_sw %.4f, 8 RHS with "
-                                      "kappa_k %s (rho_k = kappa/kappa_k - 1), one launch of 8"
+                                      "kappa_k %s (rho_k = kappa/kappa_k - 1), one launch of 8, RHS per stencil "
+                                      "thread timed"
                                       % ("x".join(map(str, L)), kappa, CSW,
                                          "-".join("%.4f" % x for x in kappas[[0, -1]])),
                           "parallelism": "replicas x%d" % world},
@@ -657,7 +659,8 @@ def run_shifts(args):
                             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 3), "peak_kind": peak_kind,
                             "algorithmic_bytes_per_launch": alg, "ms_per_launch": round(ms_b, 4),
-                            "single_rhs_ms_per_launch": round(ms_1, 4)},
+                            "single_rhs_ms_per_launch": round(ms_1, 4),
+                            "ms_per_launch_by_rhs_per_thread": ms_nbt},
                "clocks": clk.summary()}
         print(json.dumps(out))
     lat.close()

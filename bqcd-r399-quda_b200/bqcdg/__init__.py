@@ -44,7 +44,8 @@ class CgPara(C.Structure):
 
 class SolverOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("maxiter", C.c_int), ("relative", C.c_int), ("tol", C.c_double),
-                ("delta", C.c_double), ("check_true_residual", C.c_int), ("time_kernels", C.c_int)]
+                ("delta", C.c_double), ("check_true_residual", C.c_int), ("time_kernels", C.c_int),
+                ("rhs_per_thread", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -106,7 +107,7 @@ def _lib_handle():
         L.bqcdg_solve_dev.argtypes = [vp, i, i, P(Params), P(SolverOpts), P(SolveInfo)]
         L.bqcdg_mdagm_dev.argtypes = [vp, i, i, P(Params), i, i, P(C.c_double)]
         L.bqcdg_time_pass.argtypes = [vp, i, P(Params), i, i, P(C.c_double)]
-        L.bqcdg_time_pass_batch.argtypes = [vp, i, P(C.c_int), P(Params), i, i, P(C.c_double)]
+        L.bqcdg_time_pass_batch.argtypes = [vp, i, P(C.c_int), P(Params), i, i, i, P(C.c_double)]
         L.bqcdg_solve_batch.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), P(SolverOpts), i,
                                         P(SolveInfo)]
         L.bqcdg_solve_batch_shifted.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, P(SolverOpts), i,
@@ -497,11 +498,11 @@ class Lattice:
         return info
 
     def solve_batch(self, hxs, hbs, para, precision=PREC_HALF, tol=1e-10, relative=True, maxiter=100000,
-                    delta=0.1, block=0, rho=None):
+                    delta=0.1, block=0, rho=None, rhs_per_thread=0):
         """Batched mixed-precision solve of len(hxs) resident systems; block =
         right-hand sides per launch (0: autotuned).  Returns the per-RHS infos."""
         n = len(hxs)
-        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0)
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0, rhs_per_thread)
         infos = (SolveInfo * n)()
         prm = para.params(rho) if isinstance(para, HmcPara) else para
         st = lib().bqcdg_solve_batch(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm),
@@ -511,13 +512,13 @@ class Lattice:
         return list(infos)
 
     def solve_batch_shifted(self, hxs, hbs, para, rhos, precision=PREC_HALF, tol=1e-10, relative=True,
-                            maxiter=100000, delta=0.1, block=0):
+                            maxiter=100000, delta=0.1, block=0, rhs_per_thread=0):
         """solve_batch with the shift rho of system k given by rhos[k]
         (W = M~ + rho_k); the links and clover are shared."""
         n = len(hxs)
         if len(rhos) != n or len(hbs) != n:
             raise ValueError("solve_batch_shifted: one b and one rho per x")
-        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0)
+        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0, rhs_per_thread)
         infos = (SolveInfo * n)()
         prm = para.params(0.0) if isinstance(para, HmcPara) else para
         r = np.ascontiguousarray(rhos, dtype=np.float64)
@@ -539,12 +540,13 @@ class Lattice:
         _check(lib().bqcdg_time_pass(self.h, hin, C.byref(prm), precision, n, C.byref(ms)), "time_pass")
         return ms.value
 
-    def time_pass_batch(self, hins, para, precision, n, rho=None):
+    def time_pass_batch(self, hins, para, precision, n, rho=None, rhs_per_thread=0):
         """Average device ms of one batched first stencil pass over the
-        resident fields hins (one launch serves all of them)."""
+        resident fields hins (one launch serves all of them; rhs_per_thread
+        per stencil thread, 0 = the solver's timed choice)."""
         ms = C.c_double()
         prm = para.params(rho) if isinstance(para, HmcPara) else para
         k = len(hins)
-        _check(lib().bqcdg_time_pass_batch(self.h, k, (C.c_int * k)(*hins), C.byref(prm), precision, n,
-                                           C.byref(ms)), "time_pass_batch")
+        _check(lib().bqcdg_time_pass_batch(self.h, k, (C.c_int * k)(*hins), C.byref(prm), precision,
+                                           rhs_per_thread, n, C.byref(ms)), "time_pass_batch")
         return ms.value

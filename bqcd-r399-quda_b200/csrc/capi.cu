@@ -87,6 +87,7 @@ struct bqcdg_ctx {
     SpinorPtr p, t, q, rs, xs;
   } batch;
   int tuned_block[3] = {0, 0, 0};  // chosen RHS per launch, by precision
+  int tuned_nbt[3][17] = {};       // chosen RHS per stencil thread, by precision and RHS per launch
 
   void release(void* p) {
     if (!p) return;
@@ -577,17 +578,23 @@ int fp64_residual(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Spin
   return BQCDG_OK;
 }
 
+int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* ms = nullptr);
+
 // Batched mixed-precision CG over nb right-hand sides: the five kernels of a
 // sloppy iteration each serve all nb (CTAs rhs-fastest), every right-hand
 // side has its own scalars, stops and FP64 reliable updates, and a converged
-// or paused one costs its CTAs an early return only.
+// or paused one costs its CTAs an early return only.  nbt: right-hand sides
+// per stencil thread (2, 4: the register-blocked passes of dslash_multi.cu;
+// 0: timed choice).
 int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op, Prec sloppy, int maxiter,
-             const double* stop, double delta, bqcdg_solve_info* info, const double* rho = nullptr) {
+             const double* stop, double delta, bqcdg_solve_info* info, const double* rho, int nbt) {
   const Geom& g = c->g;
   int st = ensure_sloppy(c, sloppy, op.csw_kappa != 0.0);
   if (st) return st;
   if ((st = ensure_batch(c, sloppy, nb))) return st;
   auto& B = c->batch;
+  if (nbt == 0 && (st = tune_nbt(c, sloppy, op, nb, &nbt))) return st;
+  if (nbt > nb || op.h != 0.0) nbt = 1;  // the register-blocked passes take h = 0 only
   // the operator of right-hand side k: op, with its own shift when rho is given
   std::vector<OpParams> ops(nb, op);
   const double* drho = nullptr;
@@ -631,14 +638,25 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
   };
   while (running()) {
     for (int it = 0; it < batch; it++) {
-      launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
-                        nb);
-      launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
-                        c->dcg, c->stream, nb, drho);
-      launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream,
-                        nb);
-      launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
-                      c->dcg, c->stream, nb, true, drho);
+      if (nbt > 1) {
+        launch_mtil_pass1_n(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
+                            c->stream, nb, nbt);
+        launch_mtil_pass2_n(sloppy, g, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, c->dcg,
+                            c->stream, nb, drho, nbt);
+        launch_mtil_pass1_n(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
+                            c->stream, nb, nbt);
+        launch_cg_pass4_n(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
+                          c->dcg, c->stream, nb, drho, nbt);
+      } else {
+        launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
+                          c->stream, nb);
+        launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red,
+                          nullptr, c->dcg, c->stream, nb, drho);
+        launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
+                          c->stream, nb);
+        launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
+                        c->dcg, c->stream, nb, true, drho);
+      }
       launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
     }
     launches += 5 * batch;
@@ -722,8 +740,59 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
   return nan ? BQCDG_ENAN : BQCDG_OK;
 }
 
-// RHS per launch for a batch: the per-RHS time of the first stencil pass,
-// timed for 1, 4, 8 and 16 right-hand sides on the resident fields
+// device time of one batched first pass over the batch buffers: nb
+// right-hand sides, nbt of them per thread (1: one per CTA, dslash.cu)
+int time_pass1(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int nbt, int reps, float* ms) {
+  auto launch = [&]() {
+    if (nbt > 1)
+      launch_mtil_pass1_n(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
+                          c->stream, nb, nbt);
+    else
+      launch_mtil_pass1(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
+                        c->stream, nb);
+  };
+  for (int w = 0; w < 2; w++) launch();
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int r = 0; r < reps; r++) launch();
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CKL();
+  CK(cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  cudaEventElapsedTime(&t, c->ev0, c->ev1);
+  *ms = t / reps;
+  return BQCDG_OK;
+}
+
+// right-hand sides per stencil thread for launches of nb at precision p:
+// the fastest first pass of 1, 2 and 4 (timed once, then cached).  The
+// register-blocked passes need h = 0.  ms: the chosen time, when timed.
+int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* ms) {
+  int& cached = c->tuned_nbt[(int)p][nb];
+  if (cached && !ms) {
+    *nbt = cached;
+    return BQCDG_OK;
+  }
+  float best = 0.f;
+  int choice = 1;
+  for (int k : {1, 2, 4}) {
+    if (k > 1 && (k > nb || op.h != 0.0 || p == Prec::F64)) break;
+    float t;
+    int st = time_pass1(c, p, op, nb, k, 3, &t);
+    if (st) return st;
+    if (k == 1 || t < 0.98f * best) {
+      best = t;
+      choice = k;
+    }
+  }
+  cached = choice;
+  *nbt = choice;
+  if (ms) *ms = best;
+  return BQCDG_OK;
+}
+
+// RHS per launch for a batch: the per-RHS time of the first stencil pass
+// (at its best RHS per thread), timed for 1, 4, 8 and 16 right-hand sides
+// on the resident fields
 int tune_block(bqcdg_ctx* c, Prec p, const OpParams& op, int nmax, int* best) {
   const int cand[4] = {1, 4, 8, 16};
   int cap = 1;
@@ -735,20 +804,10 @@ int tune_block(bqcdg_ctx* c, Prec p, const OpParams& op, int nmax, int* best) {
   double bestt = 1e300;
   *best = 1;
   for (int k = 0; k < 4 && cand[k] <= cap; k++) {
-    int nb = cand[k];
-    for (int w = 0; w < 2; w++)
-      launch_mtil_pass1(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
-                        c->stream, nb);
-    CK(cudaEventRecord(c->ev0, c->stream));
-    for (int r = 0; r < 3; r++)
-      launch_mtil_pass1(p, c->g, false, c->batch.t, c->batch.p, gauge_of(c, p), ainv_of(c, p), op, nullptr,
-                        c->stream, nb);
-    CK(cudaEventRecord(c->ev1, c->stream));
-    CKL();
-    CK(cudaEventSynchronize(c->ev1));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    double per_rhs = ms / (3.0 * nb);
+    int nb = cand[k], nbt;
+    float ms;
+    if ((st = tune_nbt(c, p, op, nb, &nbt, &ms))) return st;
+    double per_rhs = ms / nb;
     if (per_rhs < bestt * 0.98) {
       bestt = per_rhs;
       *best = nb;
@@ -1105,6 +1164,7 @@ void bqcdg_solver_opts_default(bqcdg_solver_opts* o) {
   o->delta = 0.1;
   o->check_true_residual = 1;
   o->time_kernels = 0;
+  o->rhs_per_thread = 0;
 }
 
 // x, b device-resident; solver core + optional true-residual check
@@ -1478,6 +1538,8 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
   int st = check_op(c, p);
   if (st) return st;
   if (!o || !hx || !hb || !infos || nrhs <= 0 || block < 0 || block > kMaxRhs) return BQCDG_EINVAL;
+  if (o->rhs_per_thread != 0 && o->rhs_per_thread != 1 && o->rhs_per_thread != 2 && o->rhs_per_thread != 4)
+    return BQCDG_EINVAL;
   if (rho)
     for (int k = 0; k < nrhs; k++)
       if (!(rho[k] == rho[k])) return BQCDG_EINVAL;
@@ -1514,7 +1576,7 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
       bs[k] = field(c, hb[k0 + k]);
     }
     st = cg_batch(c, xs.data(), bs.data(), nb, op, sl, o->maxiter, stop.data() + k0, o->delta, infos + k0,
-                  rho ? rho + k0 : nullptr);
+                  rho ? rho + k0 : nullptr, o->rhs_per_thread);
     if (st) return st;
     for (int k = 0; k < nb; k++) {
       bqcdg_solve_info& in = infos[k0 + k];
@@ -1603,11 +1665,13 @@ int bqcdg_time_pass(bqcdg_ctx* c, int hin, const bqcdg_params* p, int precision,
   return BQCDG_OK;
 }
 
-int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_params* p, int precision, int n,
-                          double* ms) {
+int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_params* p, int precision,
+                          int rhs_per_thread, int n, double* ms) {
   int st = check_op(c, p);
   if (st) return st;
   if (!hin || nrhs <= 0 || nrhs > kMaxRhs || n <= 0) return BQCDG_EINVAL;
+  if (rhs_per_thread != 0 && rhs_per_thread != 1 && rhs_per_thread != 2 && rhs_per_thread != 4) return BQCDG_EINVAL;
+  if (rhs_per_thread > 1 && p->h != 0.0) return BQCDG_EUNSUPPORTED;
   for (int k = 0; k < nrhs; k++)
     if (!field(c, hin[k])) return BQCDG_EINVAL;
   Prec pr = prec_of(precision);
@@ -1619,15 +1683,12 @@ int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_pa
   auto& B = c->batch;
   for (int k = 0; k < nrhs; k++) launch_spinor_convert(c->g, pr, rhs_of(B.p, k), Prec::F64, S(field(c, hin[k])), c->stream);
   CKL();
-  CK(cudaEventRecord(c->ev0, c->stream));
-  for (int k = 0; k < n; k++)
-    launch_mtil_pass1(pr, c->g, false, B.t, B.p, gauge_of(c, pr), ainv_of(c, pr), op, nullptr, c->stream, nrhs);
-  CK(cudaEventRecord(c->ev1, c->stream));
-  CKL();
-  CK(cudaStreamSynchronize(c->stream));
+  int nbt = rhs_per_thread;
+  if (nbt == 0 && (st = tune_nbt(c, pr, op, nrhs, &nbt))) return st;
+  if (nbt > nrhs) nbt = 1;
   float t_ms = 0.f;
-  cudaEventElapsedTime(&t_ms, c->ev0, c->ev1);
-  if (ms) *ms = t_ms / n;
+  if ((st = time_pass1(c, pr, op, nrhs, nbt, n, &t_ms))) return st;
+  if (ms) *ms = t_ms;
   return BQCDG_OK;
 }
 

@@ -8,6 +8,7 @@
 // a few MB apart, well inside the 126 MB L2), and every BLAS step of CG that
 // can be is fused into the stencil epilogue.
 #include "kernels.cuh"
+#include "views.cuh"
 
 namespace bqcdg {
 
@@ -27,51 +28,6 @@ struct Occ {
   static constexpr int min_blocks = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS;
   static constexpr int min_blocks2 = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS2;
 };
-
-template <Prec P>
-__device__ __forceinline__ SpinorView<P> sview(SpinorPtr p, int stride);
-template <>
-__device__ __forceinline__ SpinorView<Prec::F64> sview<Prec::F64>(SpinorPtr p, int stride) {
-  return SpinorView<Prec::F64>{(double2*)p.v, stride};
-}
-template <>
-__device__ __forceinline__ SpinorView<Prec::F32> sview<Prec::F32>(SpinorPtr p, int stride) {
-  return SpinorView<Prec::F32>{(float4*)p.v, stride};
-}
-template <>
-__device__ __forceinline__ SpinorView<Prec::F16> sview<Prec::F16>(SpinorPtr p, int stride) {
-  return SpinorView<Prec::F16>{(int4*)p.v, p.norm, stride};
-}
-
-template <Prec P>
-__device__ __forceinline__ GaugeView<P> gview(const void* p, const Geom& g);
-template <>
-__device__ __forceinline__ GaugeView<Prec::F64> gview<Prec::F64>(const void* p, const Geom& g) {
-  return GaugeView<Prec::F64>{(double2*)p, g.stride, g.rec12};
-}
-template <>
-__device__ __forceinline__ GaugeView<Prec::F32> gview<Prec::F32>(const void* p, const Geom& g) {
-  return GaugeView<Prec::F32>{(float4*)p, g.stride};
-}
-template <>
-__device__ __forceinline__ GaugeView<Prec::F16> gview<Prec::F16>(const void* p, const Geom& g) {
-  return GaugeView<Prec::F16>{(short4*)p, g.stride};
-}
-
-template <Prec P>
-__device__ __forceinline__ CloverView<P> cview(CloverPtr p, int stride);
-template <>
-__device__ __forceinline__ CloverView<Prec::F64> cview<Prec::F64>(CloverPtr p, int stride) {
-  return CloverView<Prec::F64>{(double2*)p.v, stride};
-}
-template <>
-__device__ __forceinline__ CloverView<Prec::F32> cview<Prec::F32>(CloverPtr p, int stride) {
-  return CloverView<Prec::F32>{(float4*)p.v, stride};
-}
-template <>
-__device__ __forceinline__ CloverView<Prec::F16> cview<Prec::F16>(CloverPtr p, int stride) {
-  return CloverView<Prec::F16>{(int4*)p.v, p.norm, stride};
-}
 
 // ---------------------------------------------------------------------------
 // plain hopping term: out(e) = D_{e,o} in(o)   (d / d_dag, d/D21.F90:29-77)
@@ -413,17 +369,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
     double tot[1];
     final_sum<1>(part, red.maxblocks, tl.nsb, tot);
     if (threadIdx.x == 0) {
-      double rtr = tot[0];
-      cg->iter += 1;
-      cg->rtr_old = cg->rtr;
-      cg->rtr = rtr;
-      cg->beta = rtr / cg->rtr_old;
-      if (rtr > cg->maxr2) cg->maxr2 = rtr;
-      if (!(rtr == rtr)) cg->done = 4;  // NaN: stop, reported as an error
-      else if (rtr <= cg->stop_rtr) cg->done = 1;
-      else if (cg->iter >= cg->maxiter) cg->done = 3;
-      else if (rtr < cg->delta2 * cg->maxr2) cg->done = 2;  // reliable update (|r| < delta max|r|)
-      else if (cg->ru_every > 0 && cg->iter - cg->last_ru >= cg->ru_every) cg->done = 2;  // periodic check
+      cg_scalar_step(cg, tot[0]);
       red.counter[tl.rhs] = 0;
     }
   }

@@ -90,6 +90,20 @@ void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const 
                      cudaStream_t s, int nr = 1, bool xupd = true, const double* rho_rhs = nullptr);
 // (rho_rhs: device array of one shift rho per right-hand side, replacing
 //  op.rho, in the second passes; null: op.rho for all)
+// register-blocked batched passes (dslash_multi.cu): one thread serves one
+// site of nbt (2 or 4) right-hand sides, so each link and clover block is
+// loaded and decoded once for all of them.  Sloppy precisions (F32, F16)
+// and h = 0 only; pass 2 is the non-dagger one with the CG alpha update, and
+// pass 4 updates x (cg required for both).
+void launch_mtil_pass1_n(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
+                         CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr,
+                         int nbt);
+void launch_mtil_pass2_n(Prec p, const Geom& g, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e, const void* gauge,
+                         CloverPtr a_ee, const OpParams& op, RedScratch red, CgScalars* cg, cudaStream_t s, int nr,
+                         const double* rho_rhs, int nbt);
+void launch_cg_pass4_n(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
+                       const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
+                       cudaStream_t s, int nr, const double* rho_rhs, int nbt);
 // p = r + beta p; with x given (xupd = false above, single RHS), also the
 // x += alpha p of iteration `expect` if that iteration ran
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,

@@ -78,6 +78,8 @@ typedef struct {
   double delta;       /* reliable update when |r| < delta * max|r| since the last one */
   int check_true_residual; /* 1: recompute |b - A x|^2 in FP64 at the end */
   int time_kernels;   /* 1: time every stencil launch with CUDA events */
+  int rhs_per_thread; /* batched solves: right-hand sides each stencil thread serves
+                         (1, 2, 4; 0 = the fastest, timed once per context) */
 } bqcdg_solver_opts;
 
 typedef struct {
@@ -232,9 +234,11 @@ int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, in
  * Ainv_oo) at the given precision, n launches */
 int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precision, int n, double *ms);
 /* the same for the batched pass over nrhs right-hand sides hin[0..nrhs-1]
- * (1..16; FP32 or int16): average device time of one launch serving all */
-int bqcdg_time_pass_batch(bqcdg_ctx *ctx, int nrhs, const int *hin, const bqcdg_params *p, int precision, int n,
-                          double *ms);
+ * (1..16; FP32 or int16), rhs_per_thread of them per stencil thread (1, 2, 4;
+ * 0 = the batched solver's timed choice): average device time of one launch
+ * serving all */
+int bqcdg_time_pass_batch(bqcdg_ctx *ctx, int nrhs, const int *hin, const bqcdg_params *p, int precision,
+                          int rhs_per_thread, int n, double *ms);
 
 /* ---- resident HMC pieces ------------------------------------------------ */
 /* With these a trajectory keeps the links, the momenta and its spinor fields

@@ -176,3 +176,65 @@ def test_release_scratch_frees_and_recreates(bq):
     lat.mom_gauss()
     assert lat.mom_action() > 0
     lat.close()
+
+
+@pytest.mark.parametrize("prec", ["half", "single"])
+@pytest.mark.parametrize("nbt", [2, 4])
+def test_register_blocked_batch_matches_fp64(oracle_setup, bq, prec, nbt):
+    """The register-blocked passes (nbt right-hand sides per stencil thread,
+    one link and clover load for all of them) solve every system of a batch
+    whose size nbt does not divide (5: groups of 2+2+1 or 4+1, so some threads
+    carry absent RHS), with a shift per system: each solution equals the
+    single-system FP64 solve, and the iteration counts stay those of one RHS
+    per thread."""
+    s = oracle_setup
+    g, lat = s["g"], s["lat"]
+    para = bq.HmcPara(kappa=s["kappa"], csw=s["csw"])
+    precision = bq.PREC_HALF if prec == "half" else bq.PREC_SINGLE
+    rhos = [0.0, 0.1, 0.02, 0.3, 0.0]
+    bs = [g.gauss_spinor(0) for _ in rhos]
+    hb = [lat.field(b) for b in bs]
+    zero = np.zeros_like(bs[0])
+    runs = {}
+    for k in (1, nbt):
+        hx = [lat.field(zero) for _ in bs]
+        infos = lat.solve_batch_shifted(hx, hb, para, rhos, precision=precision, tol=1e-10, block=5,
+                                        rhs_per_thread=k)
+        runs[k] = (infos, [lat.field_get(h) for h in hx])
+    for j, rho in enumerate(rhos):
+        info = runs[nbt][0][j]
+        assert info.converged == 1 and info.true_rtr <= 1e-20 * info.b2, info.as_dict()
+        x_ref, _ = lat.solve(zero, bs[j], para, precision=bq.PREC_DOUBLE, tol=1e-12, rho=rho)
+        assert np.linalg.norm(runs[nbt][1][j] - x_ref) <= 1e-8 * np.linalg.norm(x_ref), (j, rho)
+        assert abs(info.niter - runs[1][0][j].niter) <= max(3, runs[1][0][j].niter // 20)
+
+
+@pytest.mark.parametrize("nbt", [2, 4])
+def test_register_blocked_batch_wilson(bq, nbt):
+    """c_sw = 0: the register-blocked second pass without a clover block
+    ((1 + rho) x + b D t) matches the FP64 solve of each system."""
+    L = (8, 8, 8, 8)
+    lat = bq.Lattice(L, (1, 1, 1, -1))
+    lat.ranset(11)
+    lat.conf_hot()
+    lat.conf_relax(2)
+    para = bq.HmcPara(kappa=0.12, csw=0.0)
+    rhos = [0.05, 0.0, 0.2, 0.1]
+    zero = np.zeros((lat.volh, 3, 4), np.complex128)
+    hb = []
+    for _ in rhos:
+        h = lat.field()
+        lat.field_gauss(h, 0.5)
+        hb.append(h)
+    hx = [lat.field(zero) for _ in rhos]
+    infos = lat.solve_batch_shifted(hx, hb, para, rhos, precision=bq.PREC_SINGLE, tol=1e-10, block=4,
+                                    rhs_per_thread=nbt)
+    for j, rho in enumerate(rhos):
+        assert infos[j].converged == 1, infos[j].as_dict()
+        b = lat.field_get(hb[j])
+        x_ref, _ = lat.solve(zero, b, para, precision=bq.PREC_DOUBLE, tol=1e-12, rho=rho)
+        assert np.linalg.norm(lat.field_get(hx[j]) - x_ref) <= 1e-8 * np.linalg.norm(x_ref), (j, rho)
+    # the timed batched pass runs for every choice of RHS per thread
+    for k in (0, 1, 2, 4):
+        assert lat.time_pass_batch(hx, para, bq.PREC_HALF, 2, rhs_per_thread=k) > 0
+    lat.close()
