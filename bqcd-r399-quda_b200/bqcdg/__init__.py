@@ -110,8 +110,8 @@ def _lib_handle():
         L.bqcdg_time_pass_batch.argtypes = [vp, i, P(C.c_int), P(Params), i, i, i, P(C.c_double)]
         L.bqcdg_solve_batch.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), P(SolverOpts), i,
                                         P(SolveInfo)]
-        L.bqcdg_solve_batch_shifted.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, P(SolverOpts), i,
-                                                P(SolveInfo)]
+        L.bqcdg_solve_batch_shifted.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, dp, P(SolverOpts),
+                                                i, P(SolveInfo)]
         L.bqcdg_ranset.argtypes = [vp, C.c_longlong, C.c_longlong]
         L.bqcdg_ranget.argtypes = [vp, P(C.c_longlong)]
         L.bqcdg_conf_hot.argtypes = [vp]
@@ -514,16 +514,18 @@ class Lattice:
     def solve_batch_shifted(self, hxs, hbs, para, rhos, precision=PREC_HALF, tol=1e-10, relative=True,
                             maxiter=100000, delta=0.1, block=0, rhs_per_thread=0):
         """solve_batch with the shift rho of system k given by rhos[k]
-        (W = M~ + rho_k); the links and clover are shared."""
+        (W = M~ + rho_k); the links and clover are shared.  tol: one number
+        for all systems, or one per system."""
         n = len(hxs)
         if len(rhos) != n or len(hbs) != n:
             raise ValueError("solve_batch_shifted: one b and one rho per x")
-        o = SolverOpts(precision, maxiter, int(relative), tol, delta, 1, 0, rhs_per_thread)
+        tols = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, dtype=np.float64), (n,)))
+        o = SolverOpts(precision, maxiter, int(relative), float(tols[0]), delta, 1, 0, rhs_per_thread)
         infos = (SolveInfo * n)()
         prm = para.params(0.0) if isinstance(para, HmcPara) else para
         r = np.ascontiguousarray(rhos, dtype=np.float64)
         st = lib().bqcdg_solve_batch_shifted(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm),
-                                             r.ctypes.data, C.byref(o), block, infos)
+                                             r.ctypes.data, tols.ctypes.data, C.byref(o), block, infos)
         if st not in (OK, ENOCONV):
             _check(st, "solve_batch_shifted")
         return list(infos)

@@ -390,6 +390,39 @@ struct SpinorView<Prec::F16> {
   __device__ __forceinline__ void store(int i, const Spinor<float>& s) const { store_scaled(i, s, 1.0f); }
 };
 
+// Loads of data that a pass reads once (links, clover blocks): read-only
+// path without L1 allocation, so these streamed fields leave L1 to the
+// neighbour spinors, which each site reads eight times.  (Measured at
+// 32^3x64: FP32 solves 2 % faster; int16 and FP64 unchanged.  Evict-first
+// loads, ld.global.cs, changed nothing.)
+__device__ __forceinline__ uint2 ld_once(const uint2* p) {
+  uint2 r;
+  asm("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(r.x), "=r"(r.y) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ int4 ld_once(const int4* p) {
+  int4 r;
+  asm("ld.global.nc.L1::no_allocate.v4.s32 {%0, %1, %2, %3}, [%4];"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float4 ld_once(const float4* p) {
+  float4 r;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double2 ld_once(const double2* p) {
+  double2 r;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float ld_once(const float* p) {
+  float r;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(r) : "l"(p));
+  return r;
+}
+
 // links --------------------------------------------------------------------
 template <typename R>
 __device__ __forceinline__ void reconstruct_col3(Link<R>& u) {
@@ -433,7 +466,7 @@ struct GaugeView<Prec::F64> {
       for (int c = 0; c < 2; c++)
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-          double2 t = __ldg(b + (c * 3 + r) * stride);
+          double2 t = ld_once(b + (c * 3 + r) * stride);
           u.m[r][c] = mkc(t.x, t.y);
         }
       reconstruct_col3(u);
@@ -444,7 +477,7 @@ struct GaugeView<Prec::F64> {
     for (int c = 0; c < 3; c++)
 #pragma unroll
       for (int r = 0; r < 3; r++) {
-        double2 t = __ldg(b + (c * 3 + r) * stride);
+        double2 t = ld_once(b + (c * 3 + r) * stride);
         u.m[r][c] = mkc(t.x, t.y);
       }
   }
@@ -466,7 +499,7 @@ struct GaugeView<Prec::F32> {
   int stride;
   __device__ __forceinline__ void load(int mu, int eo, int i, Link<float>& u) const {
     const float4* b = v + (size_t)((mu * 2 + eo) * 3) * stride + i;
-    float4 t0 = __ldg(b), t1 = __ldg(b + stride), t2 = __ldg(b + 2 * stride);
+    float4 t0 = ld_once(b), t1 = ld_once(b + stride), t2 = ld_once(b + 2 * stride);
     u.m[0][0] = mkc(t0.x, t0.y);
     u.m[1][0] = mkc(t0.z, t0.w);
     u.m[2][0] = mkc(t1.x, t1.y);
@@ -497,7 +530,7 @@ struct GaugeView<Prec::F16> {
   __device__ __forceinline__ void load_raw(int mu, int eo, int i, Link<float>& u, float& lsc) const {
     // one short4 = two complex entries = two 32-bit words
     const uint2* b = reinterpret_cast<const uint2*>(v) + (size_t)((mu * 2 + eo) * 3) * stride + i;
-    links16_decode(__ldg(b), __ldg(b + stride), __ldg(b + 2 * stride), u, lsc);
+    links16_decode(ld_once(b), ld_once(b + stride), ld_once(b + 2 * stride), u, lsc);
   }
   __device__ __forceinline__ void hop_link(int mu, bool, int eo, int idx, Link<float>& u, float& lsc) const {
     load_raw(mu, eo, idx, u, lsc);
@@ -541,7 +574,7 @@ struct CloverView<Prec::F64> {
   __device__ __forceinline__ void load_block(int i, int chi, cx<double> a[18]) const {
 #pragma unroll
     for (int k = 0; k < 18; k++) {
-      double2 t = __ldg(v + (chi * 18 + k) * stride + i);
+      double2 t = ld_once(v + (chi * 18 + k) * stride + i);
       a[k] = mkc(t.x, t.y);
     }
   }
@@ -559,7 +592,7 @@ struct CloverView<Prec::F32> {
   __device__ __forceinline__ void load_block(int i, int chi, cx<float> a[18]) const {
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      float4 t = __ldg(v + (chi * 9 + k) * stride + i);
+      float4 t = ld_once(v + (chi * 9 + k) * stride + i);
       a[2 * k] = mkc(t.x, t.y);
       a[2 * k + 1] = mkc(t.z, t.w);
     }
@@ -586,9 +619,9 @@ struct CloverView<Prec::F16> {
   }
   // raw int16 values; the block is raw * sc (applied to the block's output)
   __device__ __forceinline__ void load_block_raw(int i, int chi, cx<float> a[18], float& sc) const {
-    sc = __ldg(norm + i) * (1.0f / 32767.0f);
+    sc = ld_once(norm + i) * (1.0f / 32767.0f);
 #pragma unroll
-    for (int k = 0; k < 5; k++) clover16_decode(chi, k, __ldg(v + (chi * 4 + k) * stride + i), a);
+    for (int k = 0; k < 5; k++) clover16_decode(chi, k, ld_once(v + (chi * 4 + k) * stride + i), a);
   }
 };
 

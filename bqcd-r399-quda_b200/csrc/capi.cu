@@ -1532,9 +1532,11 @@ int bqcdg_solve_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const b
   return solve_resident(c, field(c, hx), field(c, hb), p, o, info);
 }
 
-// rho: one shift per right-hand side (null: p->rho for all)
+// rho: one shift per right-hand side (null: p->rho for all); tol: one
+// tolerance per right-hand side (null: o->tol for all)
 static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
-                       const double* rho, const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+                       const double* rho, const double* tol, const bqcdg_solver_opts* o, int block,
+                       bqcdg_solve_info* infos) {
   int st = check_op(c, p);
   if (st) return st;
   if (!o || !hx || !hb || !infos || nrhs <= 0 || block < 0 || block > kMaxRhs) return BQCDG_EINVAL;
@@ -1543,6 +1545,9 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
   if (rho)
     for (int k = 0; k < nrhs; k++)
       if (!(rho[k] == rho[k])) return BQCDG_EINVAL;
+  if (tol)
+    for (int k = 0; k < nrhs; k++)
+      if (!(tol[k] >= 0.0)) return BQCDG_EINVAL;
   for (int k = 0; k < nrhs; k++)
     if (!field(c, hx[k]) || !field(c, hb[k])) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
@@ -1557,14 +1562,15 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
   }
   std::vector<double> stop(nrhs);
   for (int k = 0; k < nrhs; k++) {
+    const double t = tol ? tol[k] : o->tol;
     if (o->relative) {
       launch_norm2(c->g, field(c, hb[k]), c->red, c->dres, c->stream);
       CKL();
       CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
-      stop[k] = o->tol * o->tol * c->hres[0];
+      stop[k] = t * t * c->hres[0];
     } else {
-      stop[k] = o->tol;
+      stop[k] = t;
     }
   }
   bool all_conv = true;
@@ -1594,13 +1600,14 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
 
 int bqcdg_solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
                       const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
-  return solve_batch(c, nrhs, hx, hb, p, nullptr, o, block, infos);
+  return solve_batch(c, nrhs, hx, hb, p, nullptr, nullptr, o, block, infos);
 }
 
 int bqcdg_solve_batch_shifted(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
-                              const double* rho, const bqcdg_solver_opts* o, int block, bqcdg_solve_info* infos) {
+                              const double* rho, const double* tol, const bqcdg_solver_opts* o, int block,
+                              bqcdg_solve_info* infos) {
   if (!rho) return BQCDG_EINVAL;
-  return solve_batch(c, nrhs, hx, hb, p, rho, o, block, infos);
+  return solve_batch(c, nrhs, hx, hb, p, rho, tol, o, block, infos);
 }
 
 int bqcdg_mdagm_dev(bqcdg_ctx* c, int hout, int hin, const bqcdg_params* p, int precision, int n, double* ms) {

@@ -224,9 +224,11 @@ int bqcdg_solve_batch(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, co
  * (W^+W) x_k = b_k with W = M~ + rho[k] (m_tilde.F90:63-73), the links and
  * clover shared.  These are the solves of the pseudofermion levels of
  * mass-preconditioned HMC, which differ only in rho (dsf1.F90:66 with
- * para%rho, dsf2.F90:64 with rho = 0); p->rho is ignored. */
+ * para%rho, dsf2.F90:64 with rho = 0); p->rho is ignored.  tol: one
+ * tolerance per system in the sense of o->relative (NULL: o->tol for all). */
 int bqcdg_solve_batch_shifted(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
-                              const double *rho, const bqcdg_solver_opts *o, int block, bqcdg_solve_info *infos);
+                              const double *rho, const double *tol, const bqcdg_solver_opts *o, int block,
+                              bqcdg_solve_info *infos);
 /* out = (W^+W) in with both resident, repeated n times; *ms = average device
  * time of one application (CUDA events on the context stream) */
 int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);

@@ -238,3 +238,19 @@ def test_register_blocked_batch_wilson(bq, nbt):
     for k in (0, 1, 2, 4):
         assert lat.time_pass_batch(hx, para, bq.PREC_HALF, 2, rhs_per_thread=k) > 0
     lat.close()
+
+
+def test_shifted_batch_per_rhs_tolerance(oracle_setup, bq):
+    """One tolerance per system: each stops at its own |r|/|b|, so a looser
+    system retires earlier while the others go on in the same launches."""
+    s = oracle_setup
+    g, lat = s["g"], s["lat"]
+    para = bq.HmcPara(kappa=s["kappa"], csw=s["csw"])
+    tols = [1e-5, 1e-10, 1e-7]
+    bs = [g.gauss_spinor(0) for _ in tols]
+    hb = [lat.field(b) for b in bs]
+    hx = [lat.field(np.zeros_like(bs[0])) for _ in tols]
+    infos = lat.solve_batch_shifted(hx, hb, para, [0.1] * 3, tol=tols, block=3)
+    for info, t in zip(infos, tols):
+        assert info.converged == 1 and info.true_rtr <= t * t * info.b2, info.as_dict()
+    assert infos[0].niter < infos[2].niter < infos[1].niter
