@@ -450,7 +450,8 @@ def run_hmc(args):
             recs.append(rec)
     if rank == 0:
         secs = [r["seconds"] for r in recs]
-        out = {"metric": "HMC trajectory time at 24^3x48 (N_f=2 clover, Hasenbusch, 20/5 nested leapfrog)",
+        out = {"metric": "HMC trajectory time at %s (N_f=2 clover, Hasenbusch, 20/5 nested leapfrog)"
+                         % "x".join(map(str, L)),
                "value": round(sum(secs) / len(secs), 3), "unit": "s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 1),
                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -537,7 +538,8 @@ def run_batch(args):
     dx = max(float(np.linalg.norm(lat.field_get(hxs[k]) - seq[n]["x"]) / np.linalg.norm(seq[n]["x"]))
              for n, k in (("point", 0), ("gauss", 12)))
     if rank == 0:
-        out = {"metric": "16-RHS batched CG time-to-1e-10 at 48^3x96, kappa 0.1355 (FP32 iterations)",
+        out = {"metric": "16-RHS batched CG time-to-1e-10 at %s, kappa 0.1355 (FP32 iterations)"
+                         % "x".join(map(str, L)),
                "value": round(batch_s, 3), "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
                "ms_per_step": round(1e3 * batch_s, 1), "higher_is_better": False, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64 (f32 sloppy iterations)",
@@ -633,7 +635,8 @@ def run_shifts(args):
               file=sys.stderr, flush=True)
         del xb, xr
     if rank == 0:
-        out = {"metric": "8-RHS shifted batched CG time-to-1e-10 at 64^3x128, kappa 0.136 (int16 iterations)",
+        out = {"metric": "8-RHS shifted batched CG time-to-1e-10 at %s, kappa 0.136 (int16 iterations)"
+                         % "x".join(map(str, L)),
                "value": round(batch_s, 3), "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
                "ms_per_step": round(1e3 * batch_s, 1), "higher_is_better": False, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64 (int16 sloppy iterations)",
