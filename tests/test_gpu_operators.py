@@ -10,7 +10,9 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-LATTICES = [(4, 4, 4, 4), (6, 4, 8, 4), (8, 8, 8, 8)]
+# (6,6,6,6): volh = 648, not a multiple of the 128-site blocks, odd x/2;
+# (2,4,6,4): extent 2, where the forward and backward x-neighbours coincide
+LATTICES = [(4, 4, 4, 4), (6, 4, 8, 4), (8, 8, 8, 8), (6, 6, 6, 6), (2, 4, 6, 4)]
 TOL64 = 1e-13
 
 

@@ -15,9 +15,10 @@ pytestmark = pytest.mark.gpu
 TOL = {1: 2e-6, 2: 2e-4}
 
 
-@pytest.fixture(scope="module")
-def lat(bq):
-    lt = bq.Lattice((8, 8, 8, 16), (1, 1, 1, -1))
+@pytest.fixture(scope="module", params=[(8, 8, 8, 16), (6, 6, 6, 6), (2, 4, 6, 4)],
+                ids=lambda L: "x".join(map(str, L)))
+def lat(request, bq):
+    lt = bq.Lattice(request.param, (1, 1, 1, -1))
     lt.ranset(5)
     lt.conf_hot()
     lt.conf_relax(1)
