@@ -671,15 +671,81 @@ def run_shifts(args):
         pg.destroy_process_group()
 
 
+def run_confio(args):
+    """Optional workload: BQCD's configuration files (conf.F90 conf_write /
+    conf_read with the per-slice cksum of cksum.c) for the 32^3x64 links of
+    the default workload.  The device reorders, byte-swaps and check-sums
+    each time slice in one pass; the files go to a scratch directory.  One
+    step = one write and one read of the whole configuration (805 MB of
+    slice files), wall-clock time including the file system.  The CPU
+    baseline is the oracle's numpy restatement with its C cksum, on a
+    bounded number of slices."""
+    import shutil
+    import tempfile
+    import numpy as np
+    import bqcdg as bq
+
+    world, rank, local, pg = dist_init()
+    L = lattice_of(args, "32,32,32,64")
+    lat = start_config(bq, L, local, args.cool)
+    d = tempfile.mkdtemp(prefix="bqcd_conf_")
+    base = os.path.join(d, "bqcd.001.1.1.00000")
+    nbytes = L[0] * L[1] * L[2] * L[3] * 384
+    u0 = lat.get_gauge()
+    w, r = [], []
+    for k in range(args.warmup + args.steps):
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        lat.conf_write(base)
+        t1 = time.perf_counter()
+        lat.conf_read(base + ".info")
+        t2 = time.perf_counter()
+        if k >= args.warmup:
+            w.append(allmax(pg, t1 - t0, local))
+            r.append(allmax(pg, t2 - t1, local))
+    dev = float(np.abs(lat.get_gauge() - u0).max())
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import confio
+        nsl = min(L[3], 8)
+        t0 = time.perf_counter()
+        for t in range(nsl):
+            confio.cksum(confio.slice_bytes(L, u0, t))
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(dt / nsl * L[3], 3), "unit": "s", "cores": 1, "kind": "port",
+               "sample": "%d of %d slices reordered to the file layout (numpy) and check-summed (C), scaled; "
+                         "no file system" % (nsl, L[3])}
+    shutil.rmtree(d, ignore_errors=True)
+    if rank == 0:
+        ws, rs = sum(w) / len(w), sum(r) / len(r)
+        out = {"metric": "configuration write + read time at %s (BQCD slice files with cksum)"
+                         % "x".join(map(str, L)),
+               "value": round(ws + rs, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(1e3 * (ws + rs), 1), "higher_is_better": False,
+               "scaling": "weak", "vs_baseline": None, "dtype": "u8 (f64 links)",
+               "data": "synthetic: device hot start + %d conf_relax sweep(s)" % lat.sweeps,
+               "config": {"workload": "conf_write + conf_read, lattice %s, %d slice files of %d bytes"
+                                      % ("x".join(map(str, L)), L[3], nbytes // L[3]),
+                          "parallelism": "replicas x%d" % world},
+               "write_s": round(ws, 4), "read_s": round(rs, 4),
+               "write_gbs": round(nbytes / ws / 1e9, 2), "read_gbs": round(nbytes / rs / 1e9, 2),
+               "round_trip_max_abs_diff": dev, "cpu_baseline": cpu}
+        print(json.dumps(out))
+    lat.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="solve", choices=["solve", "hmc", "batch", "shifts"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "hmc", "batch", "shifts", "confio"],
                     help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories; "
-                         "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128")
+                         "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128; "
+                         "confio: configuration files")
     ap.add_argument("--therm", type=int, default=10,
                     help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
     ap.add_argument("--ref-rhs", type=int, default=8, help="shifts: systems checked against an FP64 solve")
@@ -704,6 +770,8 @@ def main():
         run_batch(args)
     elif args.workload == "shifts":
         run_shifts(args)
+    elif args.workload == "confio":
+        run_confio(args)
     else:
         run_ours(args)
 

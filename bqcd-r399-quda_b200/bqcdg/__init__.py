@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.environ.get("BQCDG_LIB", os.path.join(HERE, "..", "lib", "libbqcdg.so"))
 
-OK, EINVAL, ECUDA, ENOCONV, ENAN, ENOGAUGE, ENOCLOVER, ENOMEM, EUNSUPPORTED, ENOTSU3, ENODEVICE = range(11)
+OK, EINVAL, ECUDA, ENOCONV, ENAN, ENOGAUGE, ENOCLOVER, ENOMEM, EUNSUPPORTED, ENOTSU3, ENODEVICE, ECHECKSUM, EIO = \
+    range(13)
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
 EVEN, ODD = 0, 1
 
@@ -57,6 +58,20 @@ class SolveInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ConfMeta(C.Structure):
+    """bqcdg_conf_meta: the ConfInfoHeader of a configuration (conf_info.F90)."""
+    _fields_ = [("run", C.c_int), ("traj", C.c_int), ("ensemble", C.c_int * 2), ("beta", C.c_double * 2),
+                ("kappa", C.c_double * 2), ("csw", C.c_double * 2), ("csw_kappa", C.c_double * 2),
+                ("h", C.c_double * 2), ("plaq_energy", C.c_double), ("L", C.c_int * 4), ("bc", C.c_int * 4)]
+
+    def as_dict(self):
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
 _LIB = None
 
 
@@ -83,6 +98,8 @@ def _lib_handle():
         L.bqcdg_clover_init.argtypes = [vp, C.c_double]
         L.bqcdg_clover_init_solver.argtypes = [vp, C.c_double]
         L.bqcdg_release_scratch.argtypes = [vp, i]
+        L.bqcdg_conf_write.argtypes = [vp, C.c_char_p, P(ConfMeta)]
+        L.bqcdg_conf_read.argtypes = [vp, C.c_char_p, P(ConfMeta)]
         L.bqcdg_clover_action.argtypes = [vp, i, P(C.c_double)]
         for n in ("bqcdg_d", "bqcdg_d_dag"):
             getattr(L, n).argtypes = [vp, i, i, dp, dp]
@@ -231,6 +248,26 @@ class Lattice:
         the solver's work vectors and staging (solver), the resident momenta,
         saved links and force buffers (hmc)."""
         _check(lib().bqcdg_release_scratch(self.h, (1 if solver else 0) | (2 if hmc else 0)), "release_scratch")
+
+    def conf_write(self, base, run=1, traj=0, ensemble=(1, 1), para=None, beta=0.0):
+        """conf_write: the resident links to BQCD's slice files <base>.<tt>.u
+        and the info file <base>.info; returns the header written."""
+        m = ConfMeta()
+        m.run, m.traj = run, traj
+        for k in range(2):
+            m.ensemble[k] = ensemble[k]
+            m.beta[k] = beta
+            if para is not None:
+                m.kappa[k], m.csw[k], m.csw_kappa[k], m.h[k] = para.kappa, para.csw, para.csw_kappa, para.h
+        _check(lib().bqcdg_conf_write(self.h, base.encode(), C.byref(m)), "conf_write")
+        return m.as_dict()
+
+    def conf_read(self, info_file):
+        """conf_read: the configuration of an info file becomes the resident
+        links; returns its header."""
+        m = ConfMeta()
+        _check(lib().bqcdg_conf_read(self.h, info_file.encode(), C.byref(m)), "conf_read")
+        return m.as_dict()
 
     def clover_init_solver(self, csw_kappa):
         """clover_init keeping only the two parts the even-odd solver uses (A

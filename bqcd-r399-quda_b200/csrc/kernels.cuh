@@ -109,6 +109,16 @@ void launch_cg_pass4_n(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, cons
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,
                        int nr = 1, SpinorPtr x = SpinorPtr{}, int expect = -1);
 
+// ---- configuration files (confio.cu) ----
+// time slice t of the resident FP64 links in the order and byte order of
+// BQCD's slice files (24 big-endian complex per site, 384 bytes), and back
+// with the third column rebuilt; *acc ^= the raw CRC register of the slice
+// (zero it first; cksum's length and complement are applied on the host)
+cudaError_t launch_links_to_file(const Geom& g, const double2* gauge, int t, void* out, unsigned* acc,
+                                 cudaStream_t s);
+cudaError_t launch_links_from_file(const Geom& g, const void* in, int t, double2* gauge, unsigned* acc,
+                                   cudaStream_t s);
+
 // ---- BLAS / conversions (blas.cu) ----
 // r = b - Ax (F64), copy r into p (precision pp); res2[0] = |r|^2, res2[1] = |b|^2
 void launch_residual(const Geom& g, double2* r, const double2* b, const double2* ax, Prec pp, SpinorPtr p,

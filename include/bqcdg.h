@@ -45,6 +45,8 @@ extern "C" {
 #define BQCDG_EUNSUPPORTED 8 /* e.g. h != 0 in the QUDA hook (invert_quda.F90:298-301) */
 #define BQCDG_ENOTSU3 9      /* links not SU(3): 12-real sloppy storage impossible */
 #define BQCDG_ENODEVICE 10   /* no CUDA device */
+#define BQCDG_ECHECKSUM 11   /* a configuration file disagrees with the check sum of its info file */
+#define BQCDG_EIO 12         /* a file could not be opened, read or written, or is not in the expected form */
 
 typedef struct bqcdg_ctx bqcdg_ctx;
 
@@ -241,6 +243,34 @@ int bqcdg_time_pass(bqcdg_ctx *ctx, int hin, const bqcdg_params *p, int precisio
  * serving all */
 int bqcdg_time_pass_batch(bqcdg_ctx *ctx, int nrhs, const int *hin, const bqcdg_params *p, int precision,
                           int rhs_per_thread, int n, double *ms);
+
+/* ---- configuration files (conf.F90:219-470) ---------------------------- */
+/* BQCD's gauge configuration format: one binary file per time slice t,
+ * <base>.<tt>.u (tt: t with at least two digits, files.F90:219-234), holding
+ * NZ records (one per z) of the sites of that slice in y, x order, each site
+ * the first two columns of its four links as 24 big-endian REAL(8) complex
+ * numbers, rows fastest, then columns, then mu (conf_seq, conf.F90:219-259;
+ * field_io, comm/field_io_mpi.F90; swap_endian8, misc.F90:197-240); and an
+ * info file <base>.info with the ConfInfoHeader block (conf_info.F90:28-63)
+ * and one line per slice file with its POSIX cksum and byte count
+ * (write_cksum, conf_info.F90:165-190; cksum.c).  On the device each slice
+ * is reordered, byte-swapped and check-summed in one pass. */
+typedef struct {
+  int run, traj;          /* Run, Traj */
+  int ensemble[2];        /* ensemble, former_ensemble */
+  double beta[2], kappa[2], csw[2], csw_kappa[2], h[2];
+  double plaq_energy;     /* PlaqEnergy = sg / (6 V); written: computed from the links */
+  int L[4], bc[4];        /* L, bc_fermions; written: the context's */
+} bqcdg_conf_meta;
+/* conf_write: the resident links to the slice files and the info file */
+int bqcdg_conf_write(bqcdg_ctx *ctx, const char *base, bqcdg_conf_meta *meta);
+/* conf_read: the configuration named by an info file becomes the resident
+ * links (the third columns rebuilt by u_complete, su3.F90:301-310).  Slice
+ * file names are taken relative to the info file's directory.  A lattice
+ * other than the context's gives BQCDG_EINVAL, a check-sum mismatch
+ * BQCDG_ECHECKSUM (conf.F90 dies in both cases); afterwards no gauge field
+ * is loaded.  meta receives the header. */
+int bqcdg_conf_read(bqcdg_ctx *ctx, const char *info_file, bqcdg_conf_meta *meta);
 
 /* ---- resident HMC pieces ------------------------------------------------ */
 /* With these a trajectory keeps the links, the momenta and its spinor fields

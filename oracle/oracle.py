@@ -37,6 +37,8 @@ def lib():
         L.oqc_ranset.argtypes = [C.c_longlong, C.c_longlong]
         L.oqc_ranget.restype = C.c_longlong
         L.oqc_ranf.restype = C.c_double
+        L.oqc_cksum.argtypes = [C.c_void_p, C.c_longlong]
+        L.oqc_cksum.restype = C.c_uint
         for n in ("oqc_conf_hot", "oqc_conf_cold", "oqc_conf_relax", "oqc_flip_bc"):
             getattr(L, n).argtypes = [vp, C.c_void_p]
         L.oqc_sg.argtypes = [vp, C.c_void_p]

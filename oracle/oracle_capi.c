@@ -129,3 +129,38 @@ void oqc_clover_dsd(const oq_geom *g, int eo, double *pgen, const double *bfield
 void oqc_dsg(const oq_geom *g, double *pgen, const double *u, double step, double beta) {
   oq_dsg(g, pgen, (const oq_cplx *)u, step, beta);
 }
+
+/* ---- configuration files: the check sum of cksum.c ---------------------
+ * POSIX.2 cksum (cksum.c:60-165): CRC with the generator polynomial
+ * 0x04C11DB7, most significant bit first, register starting at 0; after
+ * the data the byte count is fed in, least significant byte first, until
+ * it is exhausted; the result is the complement of the low 32 bits.  The
+ * byte table is generated here from the polynomial. */
+static unsigned int oqc_crc_tab[256];
+static int oqc_crc_ready = 0;
+
+static void oqc_crc_init(void) {
+  for (unsigned int b = 0; b < 256; b++) {
+    unsigned int r = b << 24;
+    for (int k = 0; k < 8; k++) r = (r & 0x80000000u) ? (r << 1) ^ 0x04C11DB7u : (r << 1);
+    oqc_crc_tab[b] = r;
+  }
+  oqc_crc_ready = 1;
+}
+
+/* raw register after n bytes, continuing from crc */
+unsigned int oqc_crc_update(unsigned int crc, const unsigned char* p, long long n) {
+  if (!oqc_crc_ready) oqc_crc_init();
+  for (long long k = 0; k < n; k++) crc = (crc << 8) ^ oqc_crc_tab[((crc >> 24) ^ p[k]) & 0xFFu];
+  return crc;
+}
+
+/* the cksum value of n bytes */
+unsigned int oqc_cksum(const unsigned char* p, long long n) {
+  unsigned int crc = oqc_crc_update(0u, p, n);
+  for (long long len = n; len > 0; len >>= 8) {
+    unsigned char b = (unsigned char)(len & 0xFF);
+    crc = oqc_crc_update(crc, &b, 1);
+  }
+  return ~crc;
+}
