@@ -97,6 +97,46 @@ static int run_hmc(const int L[4], int cold, char model, double rho, double kapp
   return 0;
 }
 
+/* work/input.test: 20 trajectories of the quick-test system, the first 10
+ * force-accepted (hmc_accept_first 10, numbered -9..0), then 10 with the
+ * Metropolis test (1..10); the %it, %fa and %mc records of mc.F90 */
+static int test20(void) {
+  const int L[4] = {4, 4, 4, 4}, bc[4] = {1, 1, 1, -1};
+  oq_hmc_para p;
+  memset(&p, 0, sizeof p);
+  p.beta = 5.0;
+  p.kappa = 0.13;
+  p.csw = 2.3327;
+  p.csw_kappa = p.csw * p.kappa;
+  p.traj_length = 0.2;
+  p.ntau = 10;
+  p.tau = p.traj_length / p.ntau;
+  p.rho = 0.1;
+  p.m_scale = 3;
+  p.model = 'C';
+  oq_run r;
+  if (oq_run_init(&r, L, bc, &p, 1, 0, 1e-5f, 1000, 0, 7)) return 1;
+  for (int k = -9; k <= 10; k++) {
+    oq_hmc_out out;
+    memset(&out, 0, sizeof out);
+    oq_hmc(&r, &out, k <= 0);
+    /* a rejected trajectory keeps the old links, whose plaquette is printed */
+    const double sg = out.accepted ? out.sg : oq_sg(&r.geom, r.conf.u);
+    printf("%%it %d %d %d\n", k, out.it_f1, out.it_f2);
+    if (k <= 0)
+      printf("%%fa %d %d %.12f %.12f %d %d %d\n", k, 1, sg / (6.0 * r.geom.volume), out.exp_dh, out.cg_ncall,
+             out.cg_niter_tot, out.cg_niter_max);
+    else
+      printf("%%mc %d %d %d %.12f %.12f %d %d %d %d\n", k, 1, 1, sg / (6.0 * r.geom.volume), out.exp_dh,
+             out.accepted, out.cg_ncall, out.cg_niter_tot, out.cg_niter_max);
+  }
+  int64_t seed;
+  oq_ranget(&seed);
+  printf("Seed %lld\n", (long long)seed);
+  oq_run_free(&r);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc < 2) {
     fprintf(stderr, "usage: %s ranf_test | quick_test | hmc ...\n", argv[0]);
@@ -111,6 +151,7 @@ int main(int argc, char **argv) {
     const int L[4] = {4, 4, 4, 4};
     return run_hmc(L, 1, 'C', 0.1, 0.13, 2.3327, 5.0, 0.2, 10, 3);
   }
+  if (!strcmp(argv[1], "test20")) return test20();
   if (!strcmp(argv[1], "hmc") && argc == 15) {
     int L[4] = {atoi(argv[2]), atoi(argv[3]), atoi(argv[4]), atoi(argv[5])};
     return run_hmc(L, !strcmp(argv[6], "cold"), argv[7][0], atof(argv[8]), atof(argv[9]), atof(argv[10]),

@@ -4,6 +4,8 @@ test outputs (run in a checkout that has the reference sources mounted):
   ranf_test.reference            -> ranf_test.json   (RNG known answers)
   work/out.quick-test.reference  -> quick_test.json  (%it/%Favg/%Fmax/%fa records
                                                       of one 4^4 HMC trajectory)
+  work/out.test.reference        -> test20.json      (%it/%fa/%mc records of 20
+                                                      trajectories, work/input.test)
 
 Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
@@ -56,6 +58,31 @@ def parse_quick(path):
     return out
 
 
+def parse_test20(path):
+    """The %it, %fa and %mc records (mc.F90) and the final seed of the
+    20-trajectory test: 10 force-accepted trajectories, then 10 with the
+    Metropolis test."""
+    recs, seed = [], None
+    for line in open(path):
+        f = line.split()
+        if not f:
+            continue
+        if f[0] == "%it":
+            recs.append({"traj": int(f[1]), "f1": int(f[2]), "f2": int(f[3])})
+        elif f[0] == "%fa":
+            recs[-1].update(kind="fa", plaq_energy=float(f[3]), exp_mdh=float(f[4]), accepted=1,
+                            cg_calls=int(f[5]), cg_it_tot=int(f[6]), cg_it_max=int(f[7]))
+        elif f[0] == "%mc":
+            recs[-1].update(kind="mc", plaq_energy=float(f[4]), exp_mdh=float(f[5]), accepted=int(f[6]),
+                            cg_calls=int(f[7]), cg_it_tot=int(f[8]), cg_it_max=int(f[9]))
+        elif f[0] == "Seed" and len(f) == 2 and int(f[1]) != 0:
+            seed = int(f[1])
+    return {"source": "work/out.test.reference:39-81 (work/input.test; BQCD 3.0.1, libd3)",
+            "records": recs, "final_seed": seed,
+            "tolerance": "floats printed with 10 decimals may differ in the last or second-last digit "
+                         "(README:235-262)"}
+
+
 def main(root):
     ranf = parse_ranf(os.path.join(root, "ranf_test.reference"))
     with open(os.path.join(HERE, "ranf_test.json"), "w") as f:
@@ -64,7 +91,10 @@ def main(root):
     quick["source"] = "work/out.quick-test.reference:39-45,50 (work/input.quick-test)"
     with open(os.path.join(HERE, "quick_test.json"), "w") as f:
         json.dump(quick, f, indent=1)
-    print("wrote", len(ranf), "ranf sections and", sorted(quick))
+    t20 = parse_test20(os.path.join(root, "work", "out.test.reference"))
+    with open(os.path.join(HERE, "test20.json"), "w") as f:
+        json.dump(t20, f, indent=1)
+    print("wrote", len(ranf), "ranf sections,", sorted(quick), "and", len(t20["records"]), "trajectories")
 
 
 if __name__ == "__main__":

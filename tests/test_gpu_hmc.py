@@ -143,3 +143,31 @@ def test_quick_test_trajectory_on_device(bq):
         assert lat.ranget() == gold["final_seed"]
     finally:
         lat.close()
+
+
+def test_twenty_trajectories_on_device(bq):
+    """work/out.test.reference: the quick-test system for 20 trajectories on
+    the device, the first 10 force-accepted and the next 10 through the
+    Metropolis test with the context's RNG stream; every record to the
+    reference's printed precision (iteration counts and CG statistics
+    exactly) and the final seed exactly."""
+    from bqcdg.hmc import Hmc
+    from test_oracle_golden import check_test20
+    with open(os.path.join(HERE, "golden", "test20.json")) as f:
+        gold = json.load(f)
+    lat = bq.Lattice(L, BC)
+    try:
+        lat.ranset(0)
+        lat.conf_cold()
+        hmc = Hmc(lat, beta=5.0, kappa=0.13, csw=2.3327, rho=0.1, traj_length=0.2, ntau=10, m_scale=3,
+                  model="C", rest=1e-5, maxiter=1000, mre_n_vec=7)
+        recs = []
+        for traj in range(-9, 11):
+            r = hmc.trajectory(force_accept=traj <= 0)
+            recs.append({"traj": traj, "f1": r["it_f1"], "f2": r["it_f2"], "plaq_energy": r["plaq_energy"],
+                         "exp_mdh": r["exp_dh"], "accepted": int(r["accepted"]), "cg_calls": r["cg_calls"],
+                         "cg_it_tot": r["cg_it_tot"], "cg_it_max": r["cg_it_max"]})
+        check_test20(recs, gold)
+        assert lat.ranget() == gold["final_seed"]
+    finally:
+        lat.close()

@@ -64,3 +64,41 @@ def test_oracle_thread_independent(oracle_exe):
         outs.append(subprocess.run([oracle_exe, "quick_test"], capture_output=True, text=True, check=True,
                                    env=env).stdout)
     assert outs[0] == outs[1]
+
+
+def check_test20(records, gold):
+    """Compare 20 trajectory records with work/out.test.reference: iteration
+    counts and CG statistics exactly, the 10-decimal plaquette and exp(-dH)
+    to the last or second-last digit (README:235-262)."""
+    assert len(records) == len(gold["records"]) == 20
+    for got, want in zip(records, gold["records"]):
+        assert got["traj"] == want["traj"]
+        assert (got["f1"], got["f2"]) == (want["f1"], want["f2"]), (got, want)
+        assert (got["cg_calls"], got["cg_it_tot"], got["cg_it_max"]) == \
+            (want["cg_calls"], want["cg_it_tot"], want["cg_it_max"]), (got, want)
+        assert got["accepted"] == want["accepted"]
+        assert abs(got["plaq_energy"] - want["plaq_energy"]) <= 2e-9, (got, want)
+        assert abs(got["exp_mdh"] - want["exp_mdh"]) <= 2e-9, (got, want)
+
+
+def test_twenty_trajectories(oracle_exe):
+    """work/out.test.reference: 10 force-accepted and 10 Metropolis
+    trajectories of the quick-test system, and the final RNG seed."""
+    gold = _golden("test20.json")
+    env = dict(os.environ, OMP_NUM_THREADS="4")
+    out = subprocess.run([oracle_exe, "test20"], capture_output=True, text=True, check=True, env=env).stdout
+    recs, seed = [], None
+    for line in out.splitlines():
+        f = line.split()
+        if f[0] == "%it":
+            recs.append({"traj": int(f[1]), "f1": int(f[2]), "f2": int(f[3])})
+        elif f[0] == "%fa":
+            recs[-1].update(plaq_energy=float(f[3]), exp_mdh=float(f[4]), accepted=1, cg_calls=int(f[5]),
+                            cg_it_tot=int(f[6]), cg_it_max=int(f[7]))
+        elif f[0] == "%mc":
+            recs[-1].update(plaq_energy=float(f[4]), exp_mdh=float(f[5]), accepted=int(f[6]), cg_calls=int(f[7]),
+                            cg_it_tot=int(f[8]), cg_it_max=int(f[9]))
+        elif f[0] == "Seed":
+            seed = int(f[1])
+    check_test20(recs, gold)
+    assert seed == gold["final_seed"]
