@@ -136,11 +136,13 @@ class Hmc:
     absolute rule rtr <= rest.  solver = "cg" is the FP64 CG of cg.F90;
     "mixed" is the path of BQCD's QUDA hook (invert_quda.F90): int16 sloppy
     iterations with FP64 reliable updates, the stop checked on the true FP64
-    residual.  A solver that does not converge raises, as cg.F90 dies unless
-    log == 2."""
+    residual.  A solver that does not converge raises, as cg.F90 dies,
+    unless cg_log == 2 (solver_ignore_no_convergence 2 of BQCD's input: the
+    FP64 CG then stops after maxiter iterations and the trajectory goes on,
+    as in the reference's benchmark inputs)."""
 
     def __init__(self, lat, beta, kappa, csw, rho, traj_length, ntau, m_scale, model="C", rest=1e-5,
-                 maxiter=1000, mre_n_vec=7, solver="cg"):
+                 maxiter=1000, mre_n_vec=7, solver="cg", cg_log=0):
         self.lat = lat
         self.beta = beta
         self.para = HmcPara(kappa=kappa, csw=csw, rho=rho)
@@ -152,6 +154,7 @@ class Hmc:
         self.hasenbusch = model != "A"
         self.rest = rest
         self.maxiter = maxiter
+        self.cg_log = cg_log
         if solver not in ("cg", "mixed"):
             raise ValueError("solver must be 'cg' or 'mixed'")
         self.solver = solver
@@ -171,7 +174,7 @@ class Hmc:
     def _solve(self, op, hx, hb):
         rho = self.para.rho if op == "w_dagger_w" else 0.0
         if self.solver == "cg":
-            it, _ = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=0, rho=rho)
+            it, _ = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=self.cg_log, rho=rho)
         else:
             from . import PREC_HALF
             info = self.lat.solve_dev(hx, hb, self.para, precision=PREC_HALF, tol=self.rest, relative=False,

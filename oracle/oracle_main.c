@@ -137,6 +137,38 @@ static int test20(void) {
   return 0;
 }
 
+/* work/input.smp: the reference's SMP benchmark, 24^3x48, model A (one
+ * pseudofermion), c_sw 1.923076923076923, one force-accepted trajectory of
+ * 10 steps with CG capped at 100 iterations (solver_rest 1e-99, which is 0
+ * in the FP32 rest; solver_ignore_no_convergence 2) and no MRE vectors */
+static int smp(void) {
+  const int L[4] = {24, 24, 24, 48}, bc[4] = {1, 1, 1, -1};
+  oq_hmc_para p;
+  memset(&p, 0, sizeof p);
+  p.beta = 5.0;
+  p.kappa = 0.13;
+  p.csw = 1.923076923076923;
+  p.csw_kappa = p.csw * p.kappa;
+  p.traj_length = 0.2;
+  p.ntau = 10;
+  p.tau = p.traj_length / p.ntau;
+  p.rho = 0.0;
+  p.m_scale = 1;
+  p.model = 'A';
+  oq_run r;
+  if (oq_run_init(&r, L, bc, &p, 1, 0, (float)1e-99, 100, 2, 0)) return 1;
+  oq_hmc_out out;
+  memset(&out, 0, sizeof out);
+  oq_hmc(&r, &out, 1);
+  int64_t seed;
+  oq_ranget(&seed);
+  printf("%%fa %d %d %.12f %.12f %d %d %d\n", 0, 1, out.sg / (6.0 * r.geom.volume), out.exp_dh, out.cg_ncall,
+         out.cg_niter_tot, out.cg_niter_max);
+  printf("Seed %lld\n", (long long)seed);
+  oq_run_free(&r);
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc < 2) {
     fprintf(stderr, "usage: %s ranf_test | quick_test | hmc ...\n", argv[0]);
@@ -152,6 +184,7 @@ int main(int argc, char **argv) {
     return run_hmc(L, 1, 'C', 0.1, 0.13, 2.3327, 5.0, 0.2, 10, 3);
   }
   if (!strcmp(argv[1], "test20")) return test20();
+  if (!strcmp(argv[1], "smp")) return smp();
   if (!strcmp(argv[1], "hmc") && argc == 15) {
     int L[4] = {atoi(argv[2]), atoi(argv[3]), atoi(argv[4]), atoi(argv[5])};
     return run_hmc(L, !strcmp(argv[6], "cold"), argv[7][0], atof(argv[8]), atof(argv[9]), atof(argv[10]),

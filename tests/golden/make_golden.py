@@ -6,6 +6,8 @@ test outputs (run in a checkout that has the reference sources mounted):
                                                       of one 4^4 HMC trajectory)
   work/out.test.reference        -> test20.json      (%it/%fa/%mc records of 20
                                                       trajectories, work/input.test)
+  work/out.smp.reference         -> smp.json         (%fa record and seed of the SMP
+                                                      benchmark, work/input.smp)
 
 Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
@@ -83,6 +85,26 @@ def parse_test20(path):
                          "(README:235-262)"}
 
 
+def parse_smp(path):
+    """The %fa record, final seed and total CPU time of the SMP benchmark
+    (24^3x48, one force-accepted trajectory, CG capped at 100 iterations)."""
+    out = {"source": "work/out.smp.reference:39,43,45,90 (work/input.smp)"}
+    for line in open(path):
+        f = line.split()
+        if not f:
+            continue
+        if f[0] == "%fa":
+            out["fa"] = {"plaq_energy": float(f[3]), "exp_mdh": float(f[4]), "cg_calls": int(f[5]),
+                         "cg_it_tot": int(f[6]), "cg_it_max": int(f[7])}
+        elif f[0] == "Seed" and len(f) == 2 and int(f[1]) != 0:
+            out["final_seed"] = int(f[1])
+        elif f[0] == "CPU-Time":
+            out["cpu_time_s"], out["cpus"] = float(f[1]), int(f[4])
+        elif f[0] == "TOTAL" and len(f) >= 3:
+            out["total_s"] = float(f[2])
+    return out
+
+
 def main(root):
     ranf = parse_ranf(os.path.join(root, "ranf_test.reference"))
     with open(os.path.join(HERE, "ranf_test.json"), "w") as f:
@@ -91,6 +113,9 @@ def main(root):
     quick["source"] = "work/out.quick-test.reference:39-45,50 (work/input.quick-test)"
     with open(os.path.join(HERE, "quick_test.json"), "w") as f:
         json.dump(quick, f, indent=1)
+    smp = parse_smp(os.path.join(root, "work", "out.smp.reference"))
+    with open(os.path.join(HERE, "smp.json"), "w") as f:
+        json.dump(smp, f, indent=1)
     t20 = parse_test20(os.path.join(root, "work", "out.test.reference"))
     with open(os.path.join(HERE, "test20.json"), "w") as f:
         json.dump(t20, f, indent=1)

@@ -171,3 +171,31 @@ def test_twenty_trajectories_on_device(bq):
         assert lat.ranget() == gold["final_seed"]
     finally:
         lat.close()
+
+
+def test_smp_benchmark_trajectory_on_device(bq):
+    """work/out.smp.reference: the reference's SMP benchmark (work/input.smp),
+    24^3x48, model A, c_sw 1.923076923076923, kappa 0.13, beta 5: one
+    force-accepted trajectory of 10 steps from a cold start with the default
+    seed, the CG capped at 100 iterations (solver_rest 1e-99, no convergence
+    ignored) and no MRE vectors.  The device run reproduces its %fa record
+    (CG statistics exactly, the plaquette to the printed precision) and the
+    final seed."""
+    from bqcdg.hmc import Hmc
+    with open(os.path.join(HERE, "golden", "smp.json")) as f:
+        gold = json.load(f)
+    lat = bq.Lattice((24, 24, 24, 48), BC)
+    try:
+        lat.ranset(0)
+        lat.conf_cold()
+        hmc = Hmc(lat, beta=5.0, kappa=0.13, csw=1.923076923076923, rho=0.0, traj_length=0.2, ntau=10, m_scale=1,
+                  model="A", rest=1e-99, maxiter=100, mre_n_vec=0, cg_log=2)
+        rec = hmc.trajectory(force_accept=True)
+        fa = gold["fa"]
+        assert (rec["cg_calls"], rec["cg_it_tot"], rec["cg_it_max"]) == (fa["cg_calls"], fa["cg_it_tot"],
+                                                                          fa["cg_it_max"]), rec
+        assert abs(rec["plaq_energy"] - fa["plaq_energy"]) <= 2e-9, rec
+        assert rec["exp_dh"] < 5e-11
+        assert lat.ranget() == gold["final_seed"]
+    finally:
+        lat.close()
