@@ -671,70 +671,92 @@ def run_shifts(args):
         pg.destroy_process_group()
 
 
-def run_smp(args):
-    """Optional workload: the reference's own SMP benchmark job, work/input.smp
-    (24^3x48, model A, kappa 0.13, c_sw 1.923076923076923, beta 5, cold start,
-    default seed, one force-accepted trajectory of 10 leapfrog steps, FP64 CG
-    capped at 100 iterations, no MRE), run on the device through the resident
-    HMC entry points.  One step = the whole job from the cold start; the value
-    is its wall time.  The job's record (CG statistics, plaquette, final seed)
-    is checked against work/out.smp.reference, which took 124.93 s on 40 CPU
-    threads.  The CPU baseline times the oracle's FP64 CG at this size on a
-    bounded number of iterations, scaled to the job's 1100."""
+# the reference's benchmark jobs (work/input.smp, work/input.mpp): beta 5,
+# kappa 0.13, c_sw 1.923076923076923, model A, tau 0.2, cold start, default
+# seed, CG capped at 100 iterations (solver_rest 1e-99, no convergence
+# ignored), no MRE vectors; the first trajectory is force-accepted
+REF_JOBS = {
+    "smp": {"L": (24, 24, 24, 48), "ntau": 10, "trajectories": 1, "threads": "40 OpenMP threads, 2012"},
+    "mpp": {"L": (48, 48, 48, 96), "ntau": 20, "trajectories": 2, "threads": "6912 MPI processes, 2011"},
+}
+
+
+def run_refjob(args, name):
+    """Optional workloads smp / mpp: the reference's own benchmark job run on
+    the device through the resident HMC entry points, from the cold start,
+    as BQCD runs it.  One step = the whole job; the value is its wall time.
+    The job's records (CG statistics, plaquette, exp(-dH), acceptance, final
+    seed) are checked against work/out.<job>.reference, whose run time is
+    printed beside.  The CPU baseline times the oracle's FP64 CG at the
+    job's size on a few iterations, scaled to the job's iteration count."""
     import numpy as np
     import bqcdg as bq
     from bqcdg.hmc import Hmc
 
+    job = REF_JOBS[name]
+    with open(os.path.join(ROOT, "tests", "golden", "%s.json" % name)) as f:
+        gold = json.load(f)
+    want = [dict(gold["fa"], accepted=1)] + gold["mc"]
     world, rank, local, pg = dist_init()
-    L = (24, 24, 24, 48)
-    gold = {"plaq_energy": 0.2512245607, "cg": [11, 1100, 100], "seed": 23583982622317, "total_s": 124.93}
-    times, rec, seed = [], None, None
+    L = job["L"]
+    csw, kappa = 1.923076923076923, 0.13
+    times, recs, seed = [], None, None
     for k in range(args.warmup + args.steps):
         lat = bq.Lattice(L, (1, 1, 1, -1), device=local)
         barrier(pg, local)
         t0 = time.perf_counter()
         lat.ranset(0)
         lat.conf_cold()
-        hmc = Hmc(lat, beta=5.0, kappa=0.13, csw=1.923076923076923, rho=0.0, traj_length=0.2, ntau=10, m_scale=1,
+        hmc = Hmc(lat, beta=5.0, kappa=kappa, csw=csw, rho=0.0, traj_length=0.2, ntau=job["ntau"], m_scale=1,
                   model="A", rest=1e-99, maxiter=100, mre_n_vec=0, cg_log=2)
-        rec = hmc.trajectory(force_accept=True)
+        recs = [hmc.trajectory(force_accept=(t == 0)) for t in range(job["trajectories"])]
         seed = lat.ranget()
         dt = allmax(pg, time.perf_counter() - t0, local)
         if k >= args.warmup:
             times.append(dt)
         lat.close()
+    ok = seed == gold["final_seed"] and len(recs) == len(want)
+    for r, w in zip(recs, want):
+        ok = ok and [r["cg_calls"], r["cg_it_tot"], r["cg_it_max"]] == [w["cg_calls"], w["cg_it_tot"],
+                                                                          w["cg_it_max"]]
+        ok = ok and int(r["accepted"]) == w["accepted"] and abs(r["plaq_energy"] - w["plaq_energy"]) <= 2e-9
     cpu = None
+    iters = sum(r["cg_it_tot"] for r in recs)
     if rank == 0 and not args.no_cpu_baseline:
+        # sampled at the SMP job's size (its host fields take 1.5 GB; the
+        # MPP job's would take 24 GB), scaled by volume and iterations
         from oracle import oracle as O
-        g = O.Geom(L, (1, 1, 1, -1))
+        Ls = REF_JOBS["smp"]["L"]
+        g = O.Geom(Ls, (1, 1, 1, -1))
         O.ranset(0)
         u = g.cold()
-        clov = g.clover_init(u, 0.13 * 1.923076923076923)
+        clov = g.clover_init(u, kappa * csw)
         b = g.gauss_spinor(0)
         n = 10
         t0 = time.perf_counter()
-        g.cg("mtdagmt", np.zeros_like(b), b, g.flip_bc(u.copy()), clov, 0.13, 0.13 * 1.923076923076923,
-             rest=0.0, maxiter=n, log=2)
+        g.cg("mtdagmt", np.zeros_like(b), b, g.flip_bc(u.copy()), clov, kappa, kappa * csw, rest=0.0, maxiter=n,
+             log=2)
         dt = time.perf_counter() - t0
-        cpu = {"value": round(dt / n * 1100, 2), "unit": "s", "cores": O.threads(), "kind": "port",
-               "sample": "%d FP64 CG iterations of the oracle at 24x24x24x48 = %.2f s, scaled to the job's 1100 "
-                         "(the CG part of the job only)" % (n, dt)}
+        scale = (L[0] * L[1] * L[2] * L[3]) / (Ls[0] * Ls[1] * Ls[2] * Ls[3])
+        cpu = {"value": round(dt / n * iters * scale, 2), "unit": "s", "cores": O.threads(), "kind": "port",
+               "sample": "%d FP64 CG iterations of the oracle at %s = %.2f s, scaled by volume (x%g) to the "
+                         "job's %d iterations (the CG part of the job only)"
+                         % (n, "x".join(map(str, Ls)), dt, scale, iters)}
     if rank == 0:
         v = sum(times) / len(times)
-        ok = ([rec["cg_calls"], rec["cg_it_tot"], rec["cg_it_max"]] == gold["cg"]
-              and abs(rec["plaq_energy"] - gold["plaq_energy"]) <= 2e-9 and seed == gold["seed"])
-        out = {"metric": "BQCD SMP benchmark job (work/input.smp) wall time on one GPU",
+        out = {"metric": "BQCD %s benchmark job (work/input.%s) wall time on one GPU" % (name.upper(), name),
                "value": round(v, 3), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": round(1e3 * v, 1), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64", "data": "the reference's own benchmark input: cold start, default seed",
-               "config": {"workload": "work/input.smp: 24x24x24x48, model A, kappa 0.13, c_sw 1.9230769, beta 5, "
-                                      "1 trajectory of 10 steps, CG capped at 100 iterations",
+               "config": {"workload": "work/input.%s: %s, model A, kappa 0.13, c_sw 1.9230769, beta 5, %d "
+                                      "trajectory(ies) of %d steps, CG capped at 100 iterations"
+                                      % (name, "x".join(map(str, L)), job["trajectories"], job["ntau"]),
                           "parallelism": "replicas x%d" % world},
-               "record": {"plaq_energy": rec["plaq_energy"], "exp_dh": rec["exp_dh"],
-                          "cg": [rec["cg_calls"], rec["cg_it_tot"], rec["cg_it_max"]], "final_seed": seed},
-               "matches_reference_record": ok,
+               "records": [{"plaq_energy": r["plaq_energy"], "exp_dh": r["exp_dh"], "accepted": bool(r["accepted"]),
+                            "cg": [r["cg_calls"], r["cg_it_tot"], r["cg_it_max"]]} for r in recs],
+               "final_seed": seed, "matches_reference_record": bool(ok),
                "reference_published_s": gold["total_s"],
-               "reference_published_hardware": "40 OpenMP threads, 2012 (work/out.smp.reference:45,90)",
+               "reference_published_hardware": "%s (work/out.%s.reference)" % (job["threads"], name),
                "cpu_baseline": cpu}
         print(json.dumps(out))
     if pg is not None:
@@ -812,10 +834,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="solve", choices=["solve", "hmc", "batch", "shifts", "confio", "smp"],
+    ap.add_argument("--workload", default="solve",
+                    choices=["solve", "hmc", "batch", "shifts", "confio", "smp", "mpp"],
                     help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories; "
                          "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128; "
-                         "confio: configuration files; smp: the reference's SMP benchmark job")
+                         "confio: configuration files; smp, mpp: the reference's benchmark jobs")
     ap.add_argument("--therm", type=int, default=10,
                     help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
     ap.add_argument("--ref-rhs", type=int, default=8, help="shifts: systems checked against an FP64 solve")
@@ -842,8 +865,8 @@ def main():
         run_shifts(args)
     elif args.workload == "confio":
         run_confio(args)
-    elif args.workload == "smp":
-        run_smp(args)
+    elif args.workload in REF_JOBS:
+        run_refjob(args, args.workload)
     else:
         run_ours(args)
 

@@ -8,6 +8,8 @@ test outputs (run in a checkout that has the reference sources mounted):
                                                       trajectories, work/input.test)
   work/out.smp.reference         -> smp.json         (%fa record and seed of the SMP
                                                       benchmark, work/input.smp)
+  work/out.mpp.reference         -> mpp.json         (%fa and %mc records and seed of
+                                                      the MPP benchmark, work/input.mpp)
 
 Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
@@ -85,10 +87,11 @@ def parse_test20(path):
                          "(README:235-262)"}
 
 
-def parse_smp(path):
-    """The %fa record, final seed and total CPU time of the SMP benchmark
-    (24^3x48, one force-accepted trajectory, CG capped at 100 iterations)."""
-    out = {"source": "work/out.smp.reference:39,43,45,90 (work/input.smp)"}
+def parse_bench(path, source):
+    """The %fa (and %mc) records, final seed and total time of a benchmark
+    job (one force-accepted trajectory, then Metropolis ones; CG capped at
+    100 iterations)."""
+    out = {"source": source, "mc": []}
     for line in open(path):
         f = line.split()
         if not f:
@@ -96,6 +99,10 @@ def parse_smp(path):
         if f[0] == "%fa":
             out["fa"] = {"plaq_energy": float(f[3]), "exp_mdh": float(f[4]), "cg_calls": int(f[5]),
                          "cg_it_tot": int(f[6]), "cg_it_max": int(f[7])}
+        elif f[0] == "%mc":
+            out["mc"].append({"traj": int(f[1]), "plaq_energy": float(f[4]), "exp_mdh": float(f[5]),
+                              "accepted": int(f[6]), "cg_calls": int(f[7]), "cg_it_tot": int(f[8]),
+                              "cg_it_max": int(f[9])})
         elif f[0] == "Seed" and len(f) == 2 and int(f[1]) != 0:
             out["final_seed"] = int(f[1])
         elif f[0] == "CPU-Time":
@@ -113,9 +120,11 @@ def main(root):
     quick["source"] = "work/out.quick-test.reference:39-45,50 (work/input.quick-test)"
     with open(os.path.join(HERE, "quick_test.json"), "w") as f:
         json.dump(quick, f, indent=1)
-    smp = parse_smp(os.path.join(root, "work", "out.smp.reference"))
-    with open(os.path.join(HERE, "smp.json"), "w") as f:
-        json.dump(smp, f, indent=1)
+    for name, lines in (("smp", "39,43,45,90"), ("mpp", "41,45,49,50,95")):
+        rec = parse_bench(os.path.join(root, "work", "out.%s.reference" % name),
+                          "work/out.%s.reference:%s (work/input.%s)" % (name, lines, name))
+        with open(os.path.join(HERE, "%s.json" % name), "w") as f:
+            json.dump(rec, f, indent=1)
     t20 = parse_test20(os.path.join(root, "work", "out.test.reference"))
     with open(os.path.join(HERE, "test20.json"), "w") as f:
         json.dump(t20, f, indent=1)

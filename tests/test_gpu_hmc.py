@@ -199,3 +199,32 @@ def test_smp_benchmark_trajectory_on_device(bq):
         assert lat.ranget() == gold["final_seed"]
     finally:
         lat.close()
+
+
+def test_mpp_benchmark_job_on_device(bq):
+    """work/out.mpp.reference: the reference's MPP benchmark (work/input.mpp,
+    run there on 6912 MPI processes), 48^3x96, model A, c_sw
+    1.923076923076923, kappa 0.13, beta 5: a force-accepted trajectory of 20
+    steps, then one through the Metropolis test, which rejects it (the links
+    go back); CG capped at 100 iterations, no MRE.  On one GPU the device run
+    reproduces both records and the final seed."""
+    from bqcdg.hmc import Hmc
+    with open(os.path.join(HERE, "golden", "mpp.json")) as f:
+        gold = json.load(f)
+    want = [dict(gold["fa"], accepted=1)] + gold["mc"]
+    lat = bq.Lattice((48, 48, 48, 96), BC)
+    try:
+        lat.ranset(0)
+        lat.conf_cold()
+        hmc = Hmc(lat, beta=5.0, kappa=0.13, csw=1.923076923076923, rho=0.0, traj_length=0.2, ntau=20, m_scale=1,
+                  model="A", rest=1e-99, maxiter=100, mre_n_vec=0, cg_log=2)
+        for k, w in enumerate(want):
+            rec = hmc.trajectory(force_accept=(k == 0))
+            assert (rec["cg_calls"], rec["cg_it_tot"], rec["cg_it_max"]) == (w["cg_calls"], w["cg_it_tot"],
+                                                                              w["cg_it_max"]), rec
+            assert int(rec["accepted"]) == w["accepted"]
+            assert abs(rec["plaq_energy"] - w["plaq_energy"]) <= 2e-9, rec
+            assert rec["exp_dh"] < 5e-11
+        assert lat.ranget() == gold["final_seed"]
+    finally:
+        lat.close()
