@@ -218,48 +218,83 @@ __device__ __forceinline__ void load_w(const Geom& g, const double2* w, int pl, 
     }
 }
 
-// clover_d_same_eo (clover_d.F90:203-231)
-__device__ void d_same_eo(double q[8], double s, const L64& u0, const L64& u1, const L64& u2, const L64& u3,
-                          const L64& u4, const L64& u5, const L64& u6, const L64& wa, const L64& wb,
-                          const L64& wc) {
-  L64 u, v, r;
-  mul2(u, u0, false, u1, false);
-  mul2(v, u3, false, u2, false);
-  mul3(r, u, false, v, true, wa, false); re_tr_j(q, r, s);
-  mul3(r, wa, false, v, false, u, true); re_tr_j(q, r, s);
-  mul3(r, u, false, wb, false, v, true); re_tr_j(q, r, s);
-  mul3(r, v, false, wb, false, u, true); re_tr_j(q, r, s);
-  mul2(u, u0, false, u6, true);
-  mul2(v, u4, true, u5, false);
-  mul3(r, wa, false, v, false, u, true); re_tr_j(q, r, -s);
-  mul3(r, u, false, v, true, wa, false); re_tr_j(q, r, -s);
-  mul3(r, v, false, wc, false, u, true); re_tr_j(q, r, -s);
-  mul3(r, u, false, wc, false, v, true); re_tr_j(q, r, -s);
+// r = op(a) op(b) op(c), one row of op(a) op(b) at a time: the same
+// products and sums as mul3, with a 3-element temporary instead of a matrix
+__device__ __forceinline__ void mul3_rows(L64& r, const L64& a, bool da, const L64& b, bool db, const L64& c,
+                                          bool dc) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    C64 t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      C64 x = el(a, i, 0, da) * el(b, 0, k, db);
+      x = x + el(a, i, 1, da) * el(b, 1, k, db);
+      t[k] = x + el(a, i, 2, da) * el(b, 2, k, db);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      C64 x = t[0] * el(c, 0, j, dc);
+      x = x + t[1] * el(c, 1, j, dc);
+      r.m[i][j] = x + t[2] * el(c, 2, j, dc);
+    }
+  }
+}
+
+// The two loops of clover_d_loop for one link and one plane.  Every link and
+// w matrix is loaded where it is used (the matrices are 36 registers each in
+// FP64; loaded together they spilled), so at most the two partial products,
+// two operands and the result are live.  The products and their order are
+// those of clover_d_same_eo / clover_d_diff_eo.
+
+// clover_d_same_eo (clover_d.F90:203-231): u0 = U_mu(a), u1 = U_nu(d),
+// u2 = U_mu(e), u3 = U_nu(a), u4 = U_nu(f), u5 = U_mu(f), u6 = U_nu(c);
+// wa = w(a), wb = w(b), wc = w(c)
+template <typename LINK, typename WLD>
+__device__ __forceinline__ void d_same_eo(double q[8], double s, const LINK& link, const WLD& wl) {
+  L64 u, v, r, x, y;
+  link(0, x); link(1, y); mul2(u, x, false, y, false);  // u0 u1
+  link(3, x); link(2, y); mul2(v, x, false, y, false);  // u3 u2
+  wl(0, x);                                               // wa
+  mul3_rows(r, u, false, v, true, x, false); re_tr_j(q, r, s);
+  mul3_rows(r, x, false, v, false, u, true); re_tr_j(q, r, s);
+  wl(1, x);                                               // wb
+  mul3_rows(r, u, false, x, false, v, true); re_tr_j(q, r, s);
+  mul3_rows(r, v, false, x, false, u, true); re_tr_j(q, r, s);
+  link(0, x); link(6, y); mul2(u, x, false, y, true);   // u0 u6^+
+  link(4, x); link(5, y); mul2(v, x, true, y, false);   // u4^+ u5
+  wl(0, x);                                               // wa
+  mul3_rows(r, x, false, v, false, u, true); re_tr_j(q, r, -s);
+  mul3_rows(r, u, false, v, true, x, false); re_tr_j(q, r, -s);
+  wl(2, x);                                               // wc
+  mul3_rows(r, v, false, x, false, u, true); re_tr_j(q, r, -s);
+  mul3_rows(r, u, false, x, false, v, true); re_tr_j(q, r, -s);
 }
 
 // clover_d_diff_eo (clover_d.F90:233-264); uuu_fwd(a,b,c) = a b^+ c^+,
-// uuu_bwd(a,b,c) = a^+ b^+ c (uuu.F90)
-__device__ void d_diff_eo(double q[8], double s, const L64& u0, const L64& u1, const L64& u2, const L64& u3,
-                          const L64& u4, const L64& u5, const L64& u6, const L64& wd, const L64& we,
-                          const L64& wf) {
-  L64 u, v, r;
-  mul3(u, u1, false, u2, true, u3, true);
-  mul3(v, u2, false, u1, true, u0, true);
-  mul3(r, u0, false, wd, false, u, false); re_tr_j(q, r, s);
-  mul3(r, u, true, wd, false, u0, true); re_tr_j(q, r, s);
-  mul3(r, v, true, we, false, u3, true); re_tr_j(q, r, s);
-  mul3(r, u3, false, we, false, v, false); re_tr_j(q, r, s);
-  mul3(u, u6, true, u5, true, u4, false);
-  mul3(v, u0, false, u6, true, u5, true);
-  mul3(r, u, true, wd, false, u0, true); re_tr_j(q, r, -s);
-  mul3(r, u0, false, wd, false, u, false); re_tr_j(q, r, -s);
-  mul3(r, u4, true, wf, false, v, true); re_tr_j(q, r, -s);
-  mul3(r, v, false, wf, false, u4, false); re_tr_j(q, r, -s);
+// uuu_bwd(a,b,c) = a^+ b^+ c (uuu.F90); wd = w(d), we = w(e), wf = w(f)
+template <typename LINK, typename WLD>
+__device__ __forceinline__ void d_diff_eo(double q[8], double s, const LINK& link, const WLD& wl) {
+  L64 u, v, r, x, y;
+  link(1, x); link(2, y); link(3, r); mul3_rows(u, x, false, y, true, r, true);  // u1 u2^+ u3^+
+  link(0, r); mul3_rows(v, y, false, x, true, r, true);                          // u2 u1^+ u0^+
+  link(0, x); wl(0, y);                                                          // u0, wd
+  mul3_rows(r, x, false, y, false, u, false); re_tr_j(q, r, s);
+  mul3_rows(r, u, true, y, false, x, true); re_tr_j(q, r, s);
+  link(3, x); wl(1, y);                                                          // u3, we
+  mul3_rows(r, v, true, y, false, x, true); re_tr_j(q, r, s);
+  mul3_rows(r, x, false, y, false, v, false); re_tr_j(q, r, s);
+  link(6, x); link(5, y); link(4, r); mul3_rows(u, x, true, y, true, r, false);  // u6^+ u5^+ u4
+  link(0, r); mul3_rows(v, r, false, x, true, y, true);                          // u0 u6^+ u5^+
+  link(0, x); wl(0, y);                                                          // u0, wd
+  mul3_rows(r, u, true, y, false, x, true); re_tr_j(q, r, -s);
+  mul3_rows(r, x, false, y, false, u, false); re_tr_j(q, r, -s);
+  link(4, x); wl(2, y);                                                          // u4, wf
+  mul3_rows(r, x, true, y, false, v, true); re_tr_j(q, r, -s);
+  mul3_rows(r, v, false, y, false, x, false); re_tr_j(q, r, -s);
 }
 
 __global__ void __launch_bounds__(kBlock) k_clover_d(Geom g, double* p, const double2* gauge, const double2* w,
                                                      int eo_w, double s) {
-  const int PMU[6] = {0, 0, 0, 1, 1, 2}, PNU[6] = {1, 2, 3, 2, 3, 3};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int me = blockIdx.y;
   if (i >= g.volh) return;
@@ -270,44 +305,41 @@ __global__ void __launch_bounds__(kBlock) k_clover_d(Geom g, double* p, const do
 #pragma unroll
   for (int k = 0; k < 8; k++) acc[k] = pp[k];
   const bool same = (e == eo_w);
-  for (int pl = 0; pl < 6; pl++) {
-    int nu;
-    double sl;
-    if (PMU[pl] == mu) { nu = PNU[pl]; sl = s; }
-    else if (PNU[pl] == mu) { nu = PMU[pl]; sl = -s; }
-    else continue;
-    // sites of clover_d_loop (clover_d.F90:175-181)
-    int xa[4], xd[4], xe[4], xf[4], xb[4], xc[4];
+  // the three planes (mu, nu) of the link, in the order of clover_d.F90:
+  // planes 0..5 are (0,1) (0,2) (0,3) (1,2) (1,3) (2,3); s for mu < nu
+#pragma unroll 1
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    const int lo = mu < nu ? mu : nu, hi = mu < nu ? nu : mu;
+    const int pl = lo == 0 ? hi - 1 : lo == 1 ? hi + 1 : 5;
+    const double sl = mu < nu ? s : -s;
+    // the corners of clover_d_loop (clover_d.F90:175-181), as shifts of
+    // a = x: d = a + mu, e = a + nu, f = a - nu, b = d + nu, c = d - nu
+    auto corner = [&](int k, int y[4]) {  // k: 0 a, 1 d, 2 e, 3 f, 4 b, 5 c
 #pragma unroll
-    for (int k = 0; k < 4; k++) xa[k] = st.x[k];
-    shift(g, xa, mu, 1, xd);
-    shift(g, xa, nu, 1, xe);
-    shift(g, xa, nu, -1, xf);
-    shift(g, xd, nu, 1, xb);
-    shift(g, xd, nu, -1, xc);
-    L64 u0, u1, u2, u3, u4, u5, u6;
-    load_link(g, gauge, mu, xa, u0);
-    load_link(g, gauge, nu, xd, u1);
-    load_link(g, gauge, mu, xe, u2);
-    load_link(g, gauge, nu, xa, u3);
-    load_link(g, gauge, nu, xf, u4);
-    load_link(g, gauge, mu, xf, u5);
-    load_link(g, gauge, nu, xc, u6);
+      for (int j = 0; j < 4; j++) y[j] = st.x[j];
+      if (k == 1 || k == 4 || k == 5) y[mu] = y[mu] + 1 == g.L[mu] ? 0 : y[mu] + 1;
+      if (k == 2 || k == 4) y[nu] = y[nu] + 1 == g.L[nu] ? 0 : y[nu] + 1;
+      if (k == 3 || k == 5) y[nu] = y[nu] == 0 ? g.L[nu] - 1 : y[nu] - 1;
+    };
+    // link k of the loop: u0 = U_mu(a), u1 = U_nu(d), u2 = U_mu(e), u3 = U_nu(a),
+    // u4 = U_nu(f), u5 = U_mu(f), u6 = U_nu(c)
+    auto link = [&](int k, L64& m) {
+      int y[4];
+      corner(k == 0 || k == 3 ? 0 : k == 1 ? 1 : k == 2 ? 2 : k == 6 ? 5 : 3, y);
+      load_link(g, gauge, (k == 0 || k == 2 || k == 5) ? mu : nu, y, m);
+    };
+    // w at the loop's corners: same parity (a, b, c), other parity (d, e, f)
+    auto wl = [&](int k, L64& m) {
+      int y[4];
+      corner(same ? (k == 0 ? 0 : k == 1 ? 4 : 5) : (k == 0 ? 1 : k == 1 ? 2 : 3), y);
+      load_w(g, w, pl, site_index(g, y), m);
+    };
     double q[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) q[k] = 0.0;
-    L64 w1, w2, w3;
-    if (same) {
-      load_w(g, w, pl, i, w1);
-      load_w(g, w, pl, site_index(g, xb), w2);
-      load_w(g, w, pl, site_index(g, xc), w3);
-      d_same_eo(q, sl, u0, u1, u2, u3, u4, u5, u6, w1, w2, w3);
-    } else {
-      load_w(g, w, pl, site_index(g, xd), w1);
-      load_w(g, w, pl, site_index(g, xe), w2);
-      load_w(g, w, pl, site_index(g, xf), w3);
-      d_diff_eo(q, sl, u0, u1, u2, u3, u4, u5, u6, w1, w2, w3);
-    }
+    if (same) d_same_eo(q, sl, link, wl);
+    else d_diff_eo(q, sl, link, wl);
 #pragma unroll
     for (int k = 0; k < 8; k++) acc[k] += q[k];
   }
