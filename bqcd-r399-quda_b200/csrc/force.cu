@@ -155,16 +155,21 @@ void launch_clover_bsa(const Geom& g, double2* w, const double2* b, const double
   k_clover_bsa<<<nblocks(g.volh), kBlock, 0, st>>>(g, w, b, a);
 }
 
-// element (k1,k2) of the full Hermitian 6x6 block from the packed slots
-__device__ __forceinline__ C64 block_el(const C64 a[18], int r, int c) {
+// element (r, c) of chiral block chi of the packed A^-1 of site i, read from
+// memory: with r, c known at compile time the slot is too, so nothing is
+// indexed at run time (a block held in an array and indexed by a loop
+// counter went to local memory)
+__device__ __forceinline__ C64 ainv_el(const double2* ainv, int stride, int i, int chi, int r, int c) {
   const int slot_up[6][6] = {{-1, 1, 2, 3, 4, 5},    {-1, -1, 6, 7, 8, 9},    {-1, -1, -1, 11, 12, 13},
                              {-1, -1, -1, -1, 14, 15}, {-1, -1, -1, -1, -1, 17}, {-1, -1, -1, -1, -1, -1}};
   if (r == c) {
     const int ds[6] = {0, 0, 10, 10, 16, 16};
-    return mkc((r & 1) ? a[ds[r]].y : a[ds[r]].x, 0.0);
+    const double2 t = __ldg(ainv + (size_t)(chi * 18 + ds[r]) * stride + i);
+    return mkc((r & 1) ? t.y : t.x, 0.0);
   }
-  if (r < c) return a[slot_up[r][c]];
-  return conjg(a[slot_up[c][r]]);
+  const int slot = r < c ? slot_up[r][c] : slot_up[c][r];
+  const double2 t = __ldg(ainv + (size_t)(chi * 18 + slot) * stride + i);
+  return r < c ? mkc(t.x, t.y) : conjg(mkc(t.x, t.y));
 }
 
 // clover_t_init.F90 + clover_ts.F90: T = (halved) A^-1 in the Dirac basis,
@@ -173,11 +178,9 @@ __device__ __forceinline__ C64 block_el(const C64 a[18], int r, int c) {
 __global__ void __launch_bounds__(kBlock) k_clover_ts(Geom g, double2* w, const double2* ainv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.volh) return;
-  C64 I1[18], I2[18];
-  CloverView<Prec::F64> A{(double2*)ainv, g.stride};
-  A.load_block(i, 0, I1);
-  A.load_block(i, 1, I2);
+#pragma unroll
   for (int c1 = 0; c1 < 3; c1++)
+#pragma unroll
     for (int c2 = 0; c2 < 3; c2++) {
       // T(s1,s2) for this colour pair
       C64 T[4][4];
@@ -186,7 +189,7 @@ __global__ void __launch_bounds__(kBlock) k_clover_ts(Geom g, double2* w, const 
 #pragma unroll
         for (int s2 = 0; s2 < 4; s2++) {
           int k1 = (s1 & 1) * 3 + c1, k2 = (s2 & 1) * 3 + c2;
-          C64 e1 = block_el(I1, k1, k2), e2 = block_el(I2, k1, k2);
+          C64 e1 = ainv_el(ainv, g.stride, i, 0, k1, k2), e2 = ainv_el(ainv, g.stride, i, 1, k1, k2);
           T[s1][s2] = ((s1 < 2) == (s2 < 2)) ? e1 + e2 : e1 - e2;
         }
       C64 r[6];
