@@ -742,6 +742,14 @@ def run_refjob(args, name):
                "sample": "%d FP64 CG iterations of the oracle at %s = %.2f s, scaled by volume (x%g) to the "
                          "job's %d iterations (the CG part of the job only)"
                          % (n, "x".join(map(str, Ls)), dt, scale, iters)}
+    # the CG bin of BQCD's timing report (timing.F90): 7728 flop per even
+    # site and iteration, over the device time of the solves
+    cg_s = sum(r["cg_seconds"] for r in recs)
+    volh = L[0] * L[1] * L[2] * L[3] // 2
+    ref_cg = gold.get("timing", {}).get("CG", {})
+    cg_line = {"calls": sum(r["cg_calls"] for r in recs), "iterations": iters, "seconds": round(cg_s, 3),
+               "gflops_bqcd_model": round(7728.0 * volh * iters / cg_s / 1e9, 1),
+               "reference_seconds": ref_cg.get("seconds"), "reference_gflops": ref_cg.get("gflops_total")}
     if rank == 0:
         v = sum(times) / len(times)
         out = {"metric": "BQCD %s benchmark job (work/input.%s) wall time on one GPU" % (name.upper(), name),
@@ -755,6 +763,7 @@ def run_refjob(args, name):
                "records": [{"plaq_energy": r["plaq_energy"], "exp_dh": r["exp_dh"], "accepted": bool(r["accepted"]),
                             "cg": [r["cg_calls"], r["cg_it_tot"], r["cg_it_max"]]} for r in recs],
                "final_seed": seed, "matches_reference_record": bool(ok),
+               "cg": cg_line,
                "reference_published_s": gold["total_s"],
                "reference_published_hardware": "%s (work/out.%s.reference)" % (job["threads"], name),
                "cpu_baseline": cpu}

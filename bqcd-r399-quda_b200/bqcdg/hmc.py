@@ -174,7 +174,7 @@ class Hmc:
     def _solve(self, op, hx, hb):
         rho = self.para.rho if op == "w_dagger_w" else 0.0
         if self.solver == "cg":
-            it, _ = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=self.cg_log, rho=rho)
+            it, info = self.lat.cg_dev(hx, hb, self.para, self.rest, maxiter=self.maxiter, log=self.cg_log, rho=rho)
         else:
             from . import PREC_HALF
             info = self.lat.solve_dev(hx, hb, self.para, precision=PREC_HALF, tol=self.rest, relative=False,
@@ -182,6 +182,7 @@ class Hmc:
             if not info.converged:
                 raise RuntimeError("mixed-precision solve did not converge: %s" % info.as_dict())
             it = info.niter
+        self.cg_seconds += info.seconds
         self.cg_ncall += 1
         self.cg_niter_tot += it
         self.cg_niter_max = max(self.cg_niter_max, it)
@@ -308,6 +309,7 @@ class Hmc:
         """hmc.F90:69-216: one trajectory; returns its record as a dict."""
         lat = self.lat
         self.cg_ncall = self.cg_niter_tot = self.cg_niter_max = 0
+        self.cg_seconds = 0.0
         self.it_f1 = self.it_f2 = 0
         self.f_count = [0.0] * 4
         self.f_avg = [0.0] * 4
@@ -330,6 +332,7 @@ class Hmc:
             "plaq_energy": (sg_new if accepted else lat.sg()) / (6.0 * self.volume),
             "it_f1": self.it_f1, "it_f2": self.it_f2,
             "cg_calls": self.cg_ncall, "cg_it_tot": self.cg_niter_tot, "cg_it_max": self.cg_niter_max,
+            "cg_seconds": self.cg_seconds,
             "f_avg": [a / c if c else a for a, c in zip(self.f_avg, self.f_count)],
             "f_max": list(self.f_max),
         }

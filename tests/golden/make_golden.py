@@ -109,6 +109,10 @@ def parse_bench(path, source):
             out["cpu_time_s"], out["cpus"] = float(f[1]), int(f[4])
         elif f[0] == "TOTAL" and len(f) >= 3:
             out["total_s"] = float(f[2])
+        elif f[0] in ("CG", "MTDAGMT", "D_TOTAL") and len(f) == 7:
+            # timing_write bins (timing.F90): calls, seconds, Mflop/s mean/min/max, Gflop/s total
+            out.setdefault("timing", {})[f[0]] = {"calls": int(f[1]), "seconds": float(f[2]),
+                                                  "gflops_total": float(f[6])}
     return out
 
 
@@ -120,7 +124,7 @@ def main(root):
     quick["source"] = "work/out.quick-test.reference:39-45,50 (work/input.quick-test)"
     with open(os.path.join(HERE, "quick_test.json"), "w") as f:
         json.dump(quick, f, indent=1)
-    for name, lines in (("smp", "39,43,45,90"), ("mpp", "41,45,49,50,95")):
+    for name, lines in (("smp", "39,43,45,58-59,74,90"), ("mpp", "41,45,49,50,63-64,79,95")):
         rec = parse_bench(os.path.join(root, "work", "out.%s.reference" % name),
                           "work/out.%s.reference:%s (work/input.%s)" % (name, lines, name))
         with open(os.path.join(HERE, "%s.json" % name), "w") as f:

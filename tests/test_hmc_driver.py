@@ -7,6 +7,7 @@ action evaluation on the last one), the model switches of hmc_integrator.F90,
 and the Gauss-Jordan solve of the MRE Gram system (mre.F90:215-279).
 """
 import math
+import types
 
 import numpy as np
 import pytest
@@ -34,7 +35,7 @@ class FakeLattice:
             if name in ("mom_action", "sg", "clover_action", "mom_change"):
                 return 1.0
             if name == "cg_dev":
-                return 10, None
+                return 10, types.SimpleNamespace(seconds=1e-3, converged=1, niter=10)
             if name == "ranf":
                 return 0.5
         return rec
