@@ -4,185 +4,9 @@
 // (plus their reduced-precision copies, rebuilt lazily after each reload),
 // scratch spinors and the reduction buffers.  Host arrays in BQCD's Fortran
 // layouts are staged with one contiguous copy and converted on the device.
-#include <cuda_runtime.h>
+#include "ctx.cuh"
 
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <ctime>
-#include <map>
-#include <string>
-#include <unistd.h>
-#include <vector>
-
-#include "../../include/bqcdg.h"
-#include "kernels.cuh"
-
-using namespace bqcdg;
-
-namespace {
-
-struct Spin64 {
-  double2* v = nullptr;
-};
-
-int status_from_cuda(cudaError_t e) {
-  if (e == cudaSuccess) return BQCDG_OK;
-  if (e == cudaErrorMemoryAllocation) return BQCDG_ENOMEM;
-  return BQCDG_ECUDA;
-}
-
-}  // namespace
-
-struct bqcdg_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  Geom g{};
-  long long bytes = 0;
-  std::vector<void*> allocations;
-  std::vector<size_t> alloc_sizes;  // bytes of allocations[k]
-
-  double2* staging = nullptr;  // Fortran-layout staging, grown on demand (stage)
-  size_t staging_bytes = 0;
-
-  double2* gauge64 = nullptr;
-  bool have_gauge = false;
-  bool gauge_su3 = false;
-  void* gauge_s[3] = {nullptr, nullptr, nullptr};  // by Prec
-  bool gauge_s_ok[3] = {false, false, false};
-  // FP64 links of the even-odd operator stored as 12 reals (SU(3) links only)
-  double2* gauge64r = nullptr;
-  bool gauge64r_ok = false;
-  Geom g12{};  // g with rec12 set
-
-  double2* A[2] = {nullptr, nullptr};
-  double2* Ainv[2] = {nullptr, nullptr};
-  double2* B[2] = {nullptr, nullptr};
-  bool have_A[2] = {false, false}, have_Ainv[2] = {false, false}, have_B[2] = {false, false};
-  CloverPtr aee_s[3], ainv_oo_s[3];
-  bool clover_s_ok[3] = {false, false, false};
-
-  std::vector<double2*> s64;
-  std::vector<SpinorPtr> s32, s16;
-
-  RedScratch red{};
-  double* dres = nullptr;        // device result scalars [16]
-  double* hres = nullptr;        // pinned mirror
-  double* drho = nullptr;        // per right-hand-side shifts of a batch [kMaxRhs]
-  CgScalars* dcg = nullptr;
-  CgScalars* hcg = nullptr;      // pinned
-
-  double* pgen = nullptr;        // device momenta (GENERATOR_FIELD layout)
-  double* mom = nullptr;         // resident momenta of the device HMC pieces
-  double* mom_old = nullptr;     // their snapshot for the force monitor
-  double2* gauge_bck = nullptr;  // saved links (restored on a rejected trajectory)
-  double2* wbuf = nullptr;       // 6 planes x 9 complex per site
-
-  std::map<int, double2*> fields;
-  int next_handle = 1;
-
-  unsigned long long seed = 48131768981101ull;  // ranf.F90:36 default seed
-
-  // batched sloppy vectors: nb right-hand sides per buffer, rsb bytes apart
-  struct Batch {
-    int cap = 0;
-    Prec prec = Prec::F64;
-    SpinorPtr p, t, q, rs, xs;
-  } batch;
-  int tuned_block[3] = {0, 0, 0};  // chosen RHS per launch, by precision
-  int tuned_nbt[3][17] = {};       // chosen RHS per stencil thread, by precision and RHS per launch
-
-  void release(void* p) {
-    if (!p) return;
-    for (size_t k = 0; k < allocations.size(); k++)
-      if (allocations[k] == p) {
-        bytes -= (long long)alloc_sizes[k];
-        allocations.erase(allocations.begin() + k);
-        alloc_sizes.erase(alloc_sizes.begin() + k);
-        break;
-      }
-    cudaFree(p);
-  }
-
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<cudaEvent_t> kev;  // kernel-timing event pairs
-
-  size_t spin_bytes(Prec p) const {
-    size_t st = (size_t)g.stride;
-    if (p == Prec::F64) return 12 * 16 * st;
-    if (p == Prec::F32) return 6 * 16 * st;
-    return 3 * 16 * st;
-  }
-
-  cudaError_t alloc(void** p, size_t n) {
-    cudaError_t e = cudaMalloc(p, n);
-    if (e == cudaSuccess) {
-      allocations.push_back(*p);
-      alloc_sizes.push_back(n);
-      bytes += (long long)n;
-    }
-    return e;
-  }
-  // the staging buffer holds at least n bytes afterwards (a spinor needs
-  // 192 B per even site, a clover parity 576 B, the links 1152 B)
-  cudaError_t stage(size_t n) {
-    if (staging_bytes >= n) return cudaSuccess;
-    release(staging);
-    staging = nullptr;
-    staging_bytes = 0;
-    cudaError_t e = alloc((void**)&staging, n);
-    if (e == cudaSuccess) staging_bytes = n;
-    return e;
-  }
-  double2* sp64(size_t k) {
-    while (s64.size() <= k) {
-      void* p = nullptr;
-      if (alloc(&p, spin_bytes(Prec::F64)) != cudaSuccess) return nullptr;
-      cudaMemsetAsync(p, 0, spin_bytes(Prec::F64), stream);
-      s64.push_back((double2*)p);
-    }
-    return s64[k];
-  }
-  SpinorPtr sp(Prec p, size_t k) {
-    if (p == Prec::F64) {
-      SpinorPtr r;
-      r.v = sp64(k);
-      return r;
-    }
-    auto& pool = p == Prec::F32 ? s32 : s16;
-    while (pool.size() <= k) {
-      SpinorPtr r;
-      if (alloc(&r.v, spin_bytes(p)) != cudaSuccess) return SpinorPtr{};
-      cudaMemsetAsync(r.v, 0, spin_bytes(p), stream);
-      if (p == Prec::F16) {
-        if (alloc((void**)&r.norm, sizeof(float) * g.stride) != cudaSuccess) return SpinorPtr{};
-        cudaMemsetAsync(r.norm, 0, sizeof(float) * g.stride, stream);
-      }
-      pool.push_back(r);
-    }
-    return pool[k];
-  }
-};
-
-namespace {
-
-SpinorPtr S(double2* p) {
-  SpinorPtr r;
-  r.v = p;
-  return r;
-}
-CloverPtr C(double2* p) {
-  CloverPtr r;
-  r.v = p;
-  return r;
-}
-
-#define CK(x)                                      \
-  do {                                             \
-    cudaError_t e_ = (x);                          \
-    if (e_ != cudaSuccess) return status_from_cuda(e_); \
-  } while (0)
-#define CKL() CK(cudaGetLastError())
+namespace bqcdg_host {
 
 int upload_spinor(bqcdg_ctx* c, const double* host, double2* dev) {
   size_t n = (size_t)c->g.volh * 12 * sizeof(double2);
@@ -819,7 +643,9 @@ int tune_block(bqcdg_ctx* c, Prec p, const OpParams& op, int nmax, int* best) {
   return BQCDG_OK;
 }
 
-}  // namespace
+}  // namespace bqcdg_host
+
+using namespace bqcdg_host;
 
 // ===========================================================================
 // C ABI
@@ -1276,13 +1102,22 @@ int bqcdg_quda_solver(bqcdg_ctx* c, double* x, const double* b, const bqcdg_para
 // ---------------------------------------------------------------------------
 // forces
 // ---------------------------------------------------------------------------
-static int ensure_force_bufs(bqcdg_ctx* c) {
+}  // extern "C"
+
+namespace bqcdg_host {
+int ensure_force_bufs(bqcdg_ctx* c) {
   if (!c->pgen) CK(c->alloc((void**)&c->pgen, (size_t)64 * c->g.volh * sizeof(double)));
   if (!c->wbuf) CK(c->alloc((void**)&c->wbuf, (size_t)54 * c->g.stride * sizeof(double2)));
   return BQCDG_OK;
 }
+}  // namespace bqcdg_host
 
-static int apply_odd_clover_inverse(bqcdg_ctx* c, double2* x) {
+extern "C" {
+
+}  // extern "C"
+
+namespace bqcdg_host {
+int apply_odd_clover_inverse(bqcdg_ctx* c, double2* x) {
   // clover_mult_b(conf%b(ODD), x) (dsf.F90:69-70); the explicit inverse when
   // only conf%i is resident
   if (c->have_B[1]) launch_clover_mult_b(c->g, x, c->B[1], c->stream);
@@ -1291,11 +1126,17 @@ static int apply_odd_clover_inverse(bqcdg_ctx* c, double2* x) {
   CKL();
   return BQCDG_OK;
 }
+}  // namespace bqcdg_host
+
+extern "C" {
 
 // dsf.F90:28-110 on device momenta p (GENERATOR_FIELD layout) from the
 // device spinors a, b: the hopping force of every link, then the clover
 // parts of both parities.  Uses scratch spinors 2 and 3.
-static int dsf_core(bqcdg_ctx* c, double* p, double step, const bqcdg_params* par, double2* da, double2* db) {
+}  // extern "C"
+
+namespace bqcdg_host {
+int dsf_core(bqcdg_ctx* c, double* p, double step, const bqcdg_params* par, double2* da, double2* db) {
   int st = ensure_force_bufs(c);
   if (st) return st;
   double2 *dat = c->sp64(2), *dbt = c->sp64(3);
@@ -1333,6 +1174,9 @@ static int dsf_core(bqcdg_ctx* c, double* p, double step, const bqcdg_params* pa
   }
   return BQCDG_OK;
 }
+}  // namespace bqcdg_host
+
+extern "C" {
 
 int bqcdg_dsf(bqcdg_ctx* c, double* p, double step, const bqcdg_params* par, const double* a, const double* b) {
   if (!c || !p || !par || !a || !b) return BQCDG_EINVAL;
@@ -1373,12 +1217,18 @@ int bqcdg_clover_dsf(bqcdg_ctx* c, int eo, double* p, const double* b, const dou
 }
 
 // clover_d.F90:40-75 on device momenta: the det-term force of parity eo
-static int dsd_core(bqcdg_ctx* c, double* p, int eo, double s) {
+}  // extern "C"
+
+namespace bqcdg_host {
+int dsd_core(bqcdg_ctx* c, double* p, int eo, double s) {
   launch_clover_ts(c->g, c->wbuf, c->Ainv[eo], c->stream);
   launch_clover_d(c->g, p, c->gauge64, c->wbuf, eo, s, c->stream);
   CKL();
   return BQCDG_OK;
 }
+}  // namespace bqcdg_host
+
+extern "C" {
 
 int bqcdg_clover_dsd(bqcdg_ctx* c, int eo, double* p, double s) {
   if (!c || !p || eo < 0 || eo > 1) return BQCDG_EINVAL;
@@ -1409,10 +1259,16 @@ int bqcdg_field_create(bqcdg_ctx* c, int* handle) {
   return BQCDG_OK;
 }
 
-static double2* field(bqcdg_ctx* c, int h) {
+}  // extern "C"
+
+namespace bqcdg_host {
+double2* field(bqcdg_ctx* c, int h) {
   auto it = c->fields.find(h);
   return it == c->fields.end() ? nullptr : it->second;
 }
+}  // namespace bqcdg_host
+
+extern "C" {
 
 int bqcdg_field_upload(bqcdg_ctx* c, int h, const double* host) {
   if (!c || !host || !field(c, h)) return BQCDG_EINVAL;
@@ -1701,433 +1557,6 @@ int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_pa
   float t_ms = 0.f;
   if ((st = time_pass1(c, pr, op, nrhs, nbt, n, &t_ms))) return st;
   if (ms) *ms = t_ms;
-  return BQCDG_OK;
-}
-
-// ---------------------------------------------------------------------------
-// resident HMC pieces: the links, the momenta and the spinor fields stay on
-// the device for a whole trajectory (hmc.F90 and the routines it calls)
-// ---------------------------------------------------------------------------
-static int ensure_mom(bqcdg_ctx* c) {
-  const size_t pn = (size_t)64 * c->g.volh * sizeof(double);
-  if (!c->mom) {
-    CK(c->alloc((void**)&c->mom, pn));
-    CK(cudaMemsetAsync(c->mom, 0, pn, c->stream));
-  }
-  if (!c->mom_old) {
-    CK(c->alloc((void**)&c->mom_old, pn));
-    CK(cudaMemsetAsync(c->mom_old, 0, pn, c->stream));
-  }
-  return BQCDG_OK;
-}
-
-// one reduction over the momentum field, returned to the host
-static int mom_sumsq(bqcdg_ctx* c, const double* a, const double* b, double* out) {
-  RedScratch r = c->red;
-  r.maxblocks = 8 * nblocks(c->g.volh);  // one partial per block, within the 64-per-block scratch
-  launch_mom_sumsq(c->g, a, b, r, c->dres, c->stream);
-  CKL();
-  CK(cudaMemcpyAsync(c->hres, c->dres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  *out = c->hres[0];
-  return BQCDG_OK;
-}
-
-// links changed on the device: cached copies are stale, the clover follows
-static int gauge_changed(bqcdg_ctx* c, double csw_kappa) {
-  for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
-  c->gauge64r_ok = false;
-  if (csw_kappa != 0.0) return bqcdg_clover_init(c, csw_kappa);
-  CK(cudaStreamSynchronize(c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_gauss(bqcdg_ctx* c) {
-  if (!c) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  int st = ensure_mom(c);
-  if (st) return st;
-  // hmc_init_p.F90:28-45: do mu; do eo: ran_gauss_volh(4, p(1,1,eo,mu), 1.0, eo)
-  const unsigned long long per = 2ull * 4ull * (unsigned long long)c->g.volh;
-  for (int me = 0; me < 8; me++) {
-    launch_ran_gauss((double2*)(c->mom + (size_t)me * c->g.volh * 8), c->g.volh, 4, 1.0, c->seed, c->stream);
-    c->seed = ranf_skip(c->seed, per);
-  }
-  CKL();
-  CK(cudaStreamSynchronize(c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_set(bqcdg_ctx* c, const double* p) {
-  if (!c || !p) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  int st = ensure_mom(c);
-  if (st) return st;
-  CK(cudaMemcpyAsync(c->mom, p, (size_t)64 * c->g.volh * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_get(bqcdg_ctx* c, double* p) {
-  if (!c || !p) return BQCDG_EINVAL;
-  if (!c->mom) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  CK(cudaMemcpyAsync(p, c->mom, (size_t)64 * c->g.volh * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_action(bqcdg_ctx* c, double* sp) {
-  if (!c || !sp || !c->mom) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  double s2 = 0.0;
-  int st = mom_sumsq(c, c->mom, nullptr, &s2);
-  if (st) return st;
-  *sp = 0.5 * s2;  // action.F90 (sp)
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_mark(bqcdg_ctx* c) {
-  if (!c || !c->mom) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  CK(cudaMemcpyAsync(c->mom_old, c->mom, (size_t)64 * c->g.volh * sizeof(double), cudaMemcpyDeviceToDevice,
-                     c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_mom_change(bqcdg_ctx* c, double* d2) {
-  if (!c || !d2 || !c->mom) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  return mom_sumsq(c, c->mom_old, c->mom, d2);
-}
-
-int bqcdg_dsg_dev(bqcdg_ctx* c, double step, double beta) {
-  if (!c || !c->mom) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  if (beta == 0.0) return BQCDG_OK;
-  CK(cudaSetDevice(c->device));
-  launch_dsg(c->g, c->gauge64, c->mom, -step * beta / 3.0, c->stream);
-  CKL();
-  return BQCDG_OK;
-}
-
-int bqcdg_hmc_u_dev(bqcdg_ctx* c, double step, double csw_kappa) {
-  if (!c || !c->mom) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  CK(cudaSetDevice(c->device));
-  launch_hmc_u(c->g, c->gauge64, c->mom, step, c->stream);
-  CKL();
-  return gauge_changed(c, csw_kappa);  // hmc_u.F90:68: clover_init of the new links
-}
-
-int bqcdg_dsf_dev(bqcdg_ctx* c, double step, const bqcdg_params* par, int ha, int hb) {
-  if (!c || !par || !c->mom || !field(c, ha) || !field(c, hb)) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  CK(cudaSetDevice(c->device));
-  return dsf_core(c, c->mom, step, par, field(c, ha), field(c, hb));
-}
-
-int bqcdg_dsd_dev(bqcdg_ctx* c, double step, const bqcdg_params* par) {
-  if (!c || !par || !c->mom) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  const double sd = -step * 2.0 * (par->csw_kappa / 8.0);  // dsd.F90:40
-  if (sd == 0.0) return BQCDG_OK;
-  if (!c->have_Ainv[1]) return BQCDG_ENOCLOVER;
-  CK(cudaSetDevice(c->device));
-  int st = ensure_force_bufs(c);
-  if (st) return st;
-  return dsd_core(c, c->mom, 1, sd);
-}
-
-int bqcdg_gauge_save(bqcdg_ctx* c) {
-  if (!c) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  CK(cudaSetDevice(c->device));
-  const size_t n = (size_t)8 * 9 * c->g.stride * sizeof(double2);
-  if (!c->gauge_bck) CK(c->alloc((void**)&c->gauge_bck, n));
-  CK(cudaMemcpyAsync(c->gauge_bck, c->gauge64, n, cudaMemcpyDeviceToDevice, c->stream));
-  return BQCDG_OK;
-}
-
-int bqcdg_gauge_restore(bqcdg_ctx* c, double csw_kappa) {
-  if (!c || !c->gauge_bck) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  const size_t n = (size_t)8 * 9 * c->g.stride * sizeof(double2);
-  CK(cudaMemcpyAsync(c->gauge64, c->gauge_bck, n, cudaMemcpyDeviceToDevice, c->stream));
-  return gauge_changed(c, csw_kappa);
-}
-
-int bqcdg_ranf(bqcdg_ctx* c, double* r) {
-  if (!c || !r) return BQCDG_EINVAL;
-  c->seed = ranf_skip(c->seed, 1);  // ranf.F90: step the 48-bit generator, then scale
-  *r = std::ldexp((double)c->seed, -48);
-  return BQCDG_OK;
-}
-
-int bqcdg_op_dev(bqcdg_ctx* c, int which, int hout, int hin, const bqcdg_params* p) {
-  int st = check_op(c, p);
-  if (st) return st;
-  if (which < 0 || which > 5 || !field(c, hout) || !field(c, hin)) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  double2 *t = c->sp64(2), *q = c->sp64(3);
-  if (!t || !q) return BQCDG_ENOMEM;
-  OpParams op = op_of(p, which >= 3);
-  SpinorPtr so = S(field(c, hout)), si = S(field(c, hin));
-  switch (which) {
-    case 0: case 3: apply_mtil(c, Prec::F64, false, so, si, S(t), op, nullptr, nullptr); break;
-    case 1: case 4: apply_mtil(c, Prec::F64, true, so, si, S(t), op, nullptr, nullptr); break;
-    default: apply_mdagm(c, Prec::F64, so, si, S(t), S(q), op);
-  }
-  CKL();
-  return BQCDG_OK;
-}
-
-int bqcdg_cg_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const bqcdg_cg_para* cgp, int* iterations,
-                 bqcdg_solve_info* info) {
-  int st = check_op(c, p);
-  if (st) return st;
-  if (!cgp || !field(c, hx) || !field(c, hb)) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  bqcdg_solve_info tmp;
-  if (!info) info = &tmp;
-  std::memset(info, 0, sizeof(*info));
-  OpParams op = op_of(p, true);
-  st = cg_core(c, field(c, hx), field(c, hb), op, Prec::F64, cgp->maxiter, (double)cgp->rest, 0.0, true, false,
-               info);
-  if (st) return st;
-  if (iterations) *iterations = info->niter;
-  if (!info->converged && cgp->log != 2) return BQCDG_ENOCONV;
-  return BQCDG_OK;
-}
-
-int bqcdg_field_cdot(bqcdg_ctx* c, int ha, int hb, double* re, double* im) {
-  if (!c || !re || !im || !field(c, ha) || !field(c, hb)) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  launch_cdot(c->g, field(c, ha), field(c, hb), c->red, c->dres, c->stream);
-  CKL();
-  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  *re = c->hres[0];
-  *im = c->hres[1];
-  return BQCDG_OK;
-}
-
-int bqcdg_field_caxpby(bqcdg_ctx* c, int hy, double ay, double are, double aim, int hx) {
-  if (!c || !field(c, hy) || !field(c, hx)) return BQCDG_EINVAL;
-  CK(cudaSetDevice(c->device));
-  launch_caxpby(c->g, are, aim, field(c, hx), ay, field(c, hy), c->stream);
-  CKL();
-  return BQCDG_OK;
-}
-
-}  // extern "C"
-
-// ---------------------------------------------------------------------------
-// configuration files (conf.F90:219-470, conf_info.F90, cksum.c)
-// ---------------------------------------------------------------------------
-namespace {
-
-// cksum's end: the byte count fed in least significant byte first, then the
-// complement (cksum.c:150-165), applied to the raw register of the data
-unsigned cksum_finish(unsigned crc, unsigned long long nbytes) {
-  static unsigned tab[256];
-  static bool ready = false;
-  if (!ready) {
-    for (unsigned b = 0; b < 256; b++) {
-      unsigned r = b << 24;
-      for (int k = 0; k < 8; k++) r = (r & 0x80000000u) ? (r << 1) ^ 0x04C11DB7u : (r << 1);
-      tab[b] = r;
-    }
-    ready = true;
-  }
-  for (unsigned long long n = nbytes; n > 0; n >>= 8) crc = (crc << 8) ^ tab[((crc >> 24) ^ (unsigned)(n & 0xFF))];
-  return ~crc;
-}
-
-std::string slice_file(const std::string& base, int t) {
-  char buf[32];
-  std::snprintf(buf, sizeof(buf), ".%02d.u", t);
-  return base + buf;
-}
-
-std::string file_part(const std::string& path) {
-  const size_t k = path.rfind('/');
-  return k == std::string::npos ? path : path.substr(k + 1);
-}
-
-std::string dir_part(const std::string& path) {
-  const size_t k = path.rfind('/');
-  return k == std::string::npos ? std::string() : path.substr(0, k + 1);
-}
-
-// pinned host buffer of one slice, released on scope exit
-struct PinnedSlice {
-  void* p = nullptr;
-  ~PinnedSlice() {
-    if (p) cudaFreeHost(p);
-  }
-};
-
-}  // namespace
-
-extern "C" {
-
-int bqcdg_conf_write(bqcdg_ctx* c, const char* base, bqcdg_conf_meta* meta) {
-  if (!c || !base || !meta) return BQCDG_EINVAL;
-  if (!c->have_gauge) return BQCDG_ENOGAUGE;
-  CK(cudaSetDevice(c->device));
-  const Geom& g = c->g;
-  const size_t nbytes = (size_t)g.L[0] * g.L[1] * g.L[2] * 384;
-  CK(c->stage(nbytes));
-  PinnedSlice host;
-  CK(cudaMallocHost(&host.p, nbytes));
-  double sg;
-  int st = bqcdg_sg(c, &sg);
-  if (st) return st;
-  meta->plaq_energy = sg / (6.0 * 2.0 * g.volh);
-  for (int d = 0; d < 4; d++) {
-    meta->L[d] = g.L[d];
-    meta->bc[d] = g.bcsign[d];
-  }
-  unsigned* acc = reinterpret_cast<unsigned*>(c->dres);
-  std::vector<unsigned> sums(g.L[3]);
-  for (int t = 0; t < g.L[3]; t++) {
-    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned), c->stream));
-    CK(launch_links_to_file(g, c->gauge64, t, c->staging, acc, c->stream));
-    CK(cudaMemcpyAsync(host.p, c->staging, nbytes, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(c->hres, acc, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    sums[t] = cksum_finish(*reinterpret_cast<unsigned*>(c->hres), nbytes);
-    FILE* f = std::fopen(slice_file(base, t).c_str(), "wb");
-    if (!f) return BQCDG_EIO;
-    const size_t w = std::fwrite(host.p, 1, nbytes, f);
-    if (std::fclose(f) != 0 || w != nbytes) return BQCDG_EIO;
-  }
-  FILE* f = std::fopen((std::string(base) + ".info").c_str(), "w");
-  if (!f) return BQCDG_EIO;
-  char host_name[64] = "unknown", date[32] = "-", clock[32] = "-";
-  gethostname(host_name, sizeof(host_name) - 1);
-  const std::time_t now = std::time(nullptr);
-  std::strftime(date, sizeof(date), "%Y-%m-%d", std::localtime(&now));
-  std::strftime(clock, sizeof(clock), "%H:%M:%S", std::localtime(&now));
-  // the ConfInfoHeader block of write_conf_info_header (conf_info.F90:28-63)
-  std::fprintf(f, " >BeginConfInfoHeader\n Format 3\n Program bqcd-b200 1\n Run %d\n Traj %d\n Host %s\n Date %s %s\n",
-               meta->run, meta->traj, host_name, date, clock);
-  std::fprintf(f, " L%3d%3d%3d%3d\n bc_fermions%3d%3d%3d%3d\n REAL_kind 8\n PlaqEnergy %25.14E\n", g.L[0], g.L[1],
-               g.L[2], g.L[3], g.bcsign[0], g.bcsign[1], g.bcsign[2], g.bcsign[3], meta->plaq_energy);
-  static const char* const pre[2] = {"", "former_"};
-  for (int k = 0; k < 2; k++) {
-    std::fprintf(f, " %sensemble %d\n", pre[k], meta->ensemble[k]);
-    std::fprintf(f, " %sbeta %.17g\n %skappa %.17g\n %scsw %.17g\n %scsw_kappa %.17g\n %sh %.17g\n", pre[k],
-                 meta->beta[k], pre[k], meta->kappa[k], pre[k], meta->csw[k], pre[k], meta->csw_kappa[k], pre[k],
-                 meta->h[k]);
-  }
-  std::fprintf(f, " >EndConfInfoHeader\n >BeginCheckSum\n");
-  for (int t = 0; t < g.L[3]; t++)
-    std::fprintf(f, " %s %u %zu\n", file_part(slice_file(base, t)).c_str(), sums[t], nbytes);
-  std::fprintf(f, " >EndCheckSum\n");
-  if (std::fclose(f) != 0) return BQCDG_EIO;
-  return BQCDG_OK;
-}
-
-int bqcdg_conf_read(bqcdg_ctx* c, const char* info_file, bqcdg_conf_meta* meta) {
-  if (!c || !info_file || !meta) return BQCDG_EINVAL;
-  std::memset(meta, 0, sizeof(*meta));
-  FILE* f = std::fopen(info_file, "r");
-  if (!f) return BQCDG_EIO;
-  // keyword lines of the header (read_keyword_*, conf_info.F90:65-90) and
-  // the CheckSum block (read_cksum, conf_info.F90:140-160)
-  std::map<std::string, std::string> keys;
-  std::vector<std::pair<std::string, unsigned long long>> files;
-  char line[1024];
-  int block = 0;  // 1 header, 2 check sums
-  while (std::fgets(line, sizeof(line), f)) {
-    char w0[512] = "", rest[512] = "";
-    if (std::sscanf(line, " %511s %511[^\n]", w0, rest) < 1) continue;
-    const std::string k(w0);
-    if (k == ">BeginConfInfoHeader") block = 1;
-    else if (k == ">BeginCheckSum") block = 2;
-    else if (k.rfind(">End", 0) == 0) block = 0;
-    else if (block == 1) keys[k] = rest;
-    else if (block == 2) {
-      unsigned long long sum = 0;
-      if (std::sscanf(rest, "%llu", &sum) != 1) {
-        std::fclose(f);
-        return BQCDG_EIO;
-      }
-      files.emplace_back(k, sum);
-    }
-  }
-  std::fclose(f);
-  auto geti = [&](const char* k, int* v, int n) {
-    auto it = keys.find(k);
-    if (it == keys.end()) return false;
-    const char* p = it->second.c_str();
-    for (int j = 0; j < n; j++) {
-      int used = 0;
-      if (std::sscanf(p, "%d%n", &v[j], &used) != 1) return false;
-      p += used;
-    }
-    return true;
-  };
-  auto getd = [&](const char* k, double* v) {
-    auto it = keys.find(k);
-    return it != keys.end() && std::sscanf(it->second.c_str(), "%lf", v) == 1;
-  };
-  int format = 0, rkind = 0;
-  if (!geti("Format", &format, 1) || format != 3) return BQCDG_EIO;  // conf_info_version (module_bqcd.F90:38)
-  if (!geti("L", meta->L, 4) || !geti("bc_fermions", meta->bc, 4) || !geti("REAL_kind", &rkind, 1) || rkind != 8)
-    return BQCDG_EIO;
-  geti("Run", &meta->run, 1);
-  geti("Traj", &meta->traj, 1);
-  getd("PlaqEnergy", &meta->plaq_energy);
-  static const char* const pre[2] = {"", "former_"};
-  for (int k = 0; k < 2; k++) {
-    const std::string p(pre[k]);
-    geti((p + "ensemble").c_str(), &meta->ensemble[k], 1);
-    getd((p + "beta").c_str(), &meta->beta[k]);
-    getd((p + "kappa").c_str(), &meta->kappa[k]);
-    getd((p + "csw").c_str(), &meta->csw[k]);
-    getd((p + "csw_kappa").c_str(), &meta->csw_kappa[k]);
-    getd((p + "h").c_str(), &meta->h[k]);
-  }
-  const Geom& g = c->g;
-  for (int d = 0; d < 4; d++)
-    if (meta->L[d] != g.L[d]) return BQCDG_EINVAL;  // check_conf_info_header (conf_info.F90:96-101)
-  if ((int)files.size() != g.L[3]) return BQCDG_EIO;
-  CK(cudaSetDevice(c->device));
-  if (!c->gauge64) CK(c->alloc((void**)&c->gauge64, (size_t)8 * 9 * g.stride * sizeof(double2)));
-  const size_t nbytes = (size_t)g.L[0] * g.L[1] * g.L[2] * 384;
-  CK(c->stage(nbytes));
-  PinnedSlice host;
-  CK(cudaMallocHost(&host.p, nbytes));
-  // the links are overwritten slice by slice: until all check out, none is loaded
-  c->have_gauge = false;
-  for (int k = 0; k < 3; k++) c->gauge_s_ok[k] = false;
-  c->gauge64r_ok = false;
-  const std::string dir = dir_part(info_file);
-  unsigned* acc = reinterpret_cast<unsigned*>(c->dres);
-  for (int t = 0; t < g.L[3]; t++) {
-    const std::string name = files[t].first[0] == '/' ? files[t].first : dir + files[t].first;
-    FILE* s = std::fopen(name.c_str(), "rb");
-    if (!s) return BQCDG_EIO;
-    const size_t r = std::fread(host.p, 1, nbytes, s);
-    const bool extra = std::fgetc(s) != EOF;
-    std::fclose(s);
-    if (r != nbytes || extra) return BQCDG_EIO;
-    CK(cudaMemcpyAsync(c->staging, host.p, nbytes, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned), c->stream));
-    CK(launch_links_from_file(g, c->staging, t, c->gauge64, acc, c->stream));
-    CK(cudaMemcpyAsync(c->hres, acc, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (cksum_finish(*reinterpret_cast<unsigned*>(c->hres), nbytes) != files[t].second) return BQCDG_ECHECKSUM;
-  }
-  launch_gauge_check(g, c->gauge64, c->red, c->dres, c->stream);
-  CKL();
-  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  c->gauge_su3 = c->hres[0] < 1e-10 && c->hres[1] < 1e-10;
-  c->have_gauge = true;
   return BQCDG_OK;
 }
 
