@@ -742,6 +742,8 @@ int bqcdg_release_scratch(bqcdg_ctx* c, int what) {
     c->release(c->staging);
     c->staging = nullptr;
     c->staging_bytes = 0;
+    c->release(c->clov_tmp);
+    c->clov_tmp = nullptr;
     for (double2* p : c->s64) c->release(p);
     c->s64.clear();
     for (std::vector<SpinorPtr>* pool : {&c->s32, &c->s16}) {
@@ -871,7 +873,8 @@ int bqcdg_clover_init(bqcdg_ctx* c, double csw_kappa) {
     if (!c->Ainv[eo]) CK(c->alloc((void**)&c->Ainv[eo], n));
     if (!c->B[eo]) CK(c->alloc((void**)&c->B[eo], n));
   }
-  launch_clover_init(c->g, c->gauge64, csw_kappa, c->A, c->Ainv, c->B, c->stream);
+  if (!c->clov_tmp) CK(c->alloc((void**)&c->clov_tmp, (size_t)54 * clover_init_chunk(c->g) * sizeof(double2)));
+  launch_clover_init(c->g, c->gauge64, csw_kappa, c->A, c->Ainv, c->B, c->clov_tmp, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   for (int eo = 0; eo < 2; eo++) c->have_A[eo] = c->have_Ainv[eo] = c->have_B[eo] = true;
@@ -896,7 +899,8 @@ int bqcdg_clover_init_solver(bqcdg_ctx* c, double csw_kappa) {
   double2* a[2] = {c->A[0], nullptr};
   double2* ai[2] = {nullptr, c->Ainv[1]};
   double2* b[2] = {nullptr, nullptr};
-  launch_clover_init(c->g, c->gauge64, csw_kappa, a, ai, b, c->stream);
+  if (!c->clov_tmp) CK(c->alloc((void**)&c->clov_tmp, (size_t)54 * clover_init_chunk(c->g) * sizeof(double2)));
+  launch_clover_init(c->g, c->gauge64, csw_kappa, a, ai, b, c->clov_tmp, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   c->have_A[0] = c->have_Ainv[1] = true;

@@ -9,64 +9,6 @@
 
 namespace bqcdg {
 
-// f(mu,nu) at site x (coordinates xs); closed loops, so periodic links
-__device__ void clover_f_mu_nu(const Geom& g, const double2* gauge, L64& f, int mu, int nu, const int xs[4]) {
-  int xp_[4], xm_[4], x_p[4], x_m[4], xmp[4], xmm[4], xpm[4];
-  shift(g, xs, mu, 1, xp_);
-  shift(g, xs, mu, -1, xm_);
-  shift(g, xs, nu, 1, x_p);
-  shift(g, xs, nu, -1, x_m);
-  shift(g, xm_, nu, 1, xmp);
-  shift(g, xm_, nu, -1, xmm);
-  shift(g, xp_, nu, -1, xpm);
-  L64 a, b, c, d, t, r;
-  lzero(f);
-  // uuuu1: u1 u2 u3^+ u4^+
-  load_link(g, gauge, mu, xs, a); load_link(g, gauge, nu, xp_, b); load_link(g, gauge, mu, x_p, c);
-  load_link(g, gauge, nu, xs, d);
-  mul2(t, a, false, b, false); mul3(r, t, false, c, true, d, true);
-#pragma unroll
-  for (int p = 0; p < 3; p++)
-#pragma unroll
-    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
-  // uuuu2: u1 u2^+ u3^+ u4
-  load_link(g, gauge, nu, xs, a); load_link(g, gauge, mu, xmp, b); load_link(g, gauge, nu, xm_, c);
-  load_link(g, gauge, mu, xm_, d);
-  mul2(t, a, false, b, true); mul3(r, t, false, c, true, d, false);
-#pragma unroll
-  for (int p = 0; p < 3; p++)
-#pragma unroll
-    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
-  // uuuu3: u1^+ u2^+ u3 u4
-  load_link(g, gauge, mu, xm_, a); load_link(g, gauge, nu, xmm, b); load_link(g, gauge, mu, xmm, c);
-  load_link(g, gauge, nu, x_m, d);
-  mul2(t, a, true, b, true); mul3(r, t, false, c, false, d, false);
-#pragma unroll
-  for (int p = 0; p < 3; p++)
-#pragma unroll
-    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
-  // uuuu4: u1^+ u2 u3 u4^+
-  load_link(g, gauge, nu, x_m, a); load_link(g, gauge, mu, x_m, b); load_link(g, gauge, nu, xpm, c);
-  load_link(g, gauge, mu, xs, d);
-  mul2(t, a, true, b, false); mul3(r, t, false, c, false, d, true);
-#pragma unroll
-  for (int p = 0; p < 3; p++)
-#pragma unroll
-    for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
-  // clover_f_mu_nu.F90:92-102
-  C64 f10 = f.m[1][0], f20 = f.m[2][0], f21 = f.m[2][1];
-  f.m[0][0] = mkc(2.0 * f.m[0][0].y, 0.0);
-  f.m[1][1] = mkc(2.0 * f.m[1][1].y, 0.0);
-  f.m[2][2] = mkc(2.0 * f.m[2][2].y, 0.0);
-  f.m[0][1] = itimes(conjg(f10) - f.m[0][1]);
-  f.m[0][2] = itimes(conjg(f20) - f.m[0][2]);
-  f.m[1][2] = itimes(conjg(f21) - f.m[1][2]);
-  f.m[1][0] = conjg(f.m[0][1]);
-  f.m[2][0] = conjg(f.m[0][2]);
-  f.m[2][1] = conjg(f.m[1][2]);
-}
-
-// full 6x6 Hermitian block (upper triangle + real diagonal used)
 struct Blk {
   C64 m[6][6];
 };
@@ -156,45 +98,152 @@ __device__ void block_inv(const Blk& a, double2* A, double2* Ainv, double2* B, i
   store_packed(Ainv, stride, i, chi, inv, 0.5);
 }
 
-__global__ void __launch_bounds__(64) k_clover_init(Geom g, const double2* gauge, double factor, double2* a0,
-                                                    double2* a1, double2* ai0, double2* ai1, double2* b0,
-                                                    double2* b1) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int eo = blockIdx.y;
-  if (i >= g.volh) return;
-  if (!(eo == 0 ? (a0 || ai0 || b0) : (a1 || ai1 || b1))) return;  // nothing wanted of this parity
-  Site st = site_coords(g, i, eo);
-  Blk p, q;
-  L64 f, f2;
-  // clover_init.F90:52-77 (1-based planes 21; 32,31; 34; 14,42)
-  clover_f_mu_nu(g, gauge, f, 1, 0, st.x);
-  init1(p, f);
-  clover_f_mu_nu(g, gauge, f, 2, 1, st.x);
-  clover_f_mu_nu(g, gauge, f2, 2, 0, st.x);
-  init2(p, f, f2);
-  clover_f_mu_nu(g, gauge, f, 2, 3, st.x);
-  init1(q, f);
-  clover_f_mu_nu(g, gauge, f, 0, 3, st.x);
-  clover_f_mu_nu(g, gauge, f2, 3, 1, st.x);
-  init2(q, f, f2);
-  // clover_init3: a1 = s(p+q)+1, a2 = s(p-q)+1 (upper triangle)
-  Blk bl;
-  double2* A = eo == 0 ? a0 : a1;
-  double2* AI = eo == 0 ? ai0 : ai1;
-  double2* B = eo == 0 ? b0 : b1;
-  for (int chi = 0; chi < 2; chi++) {
-    const double sg = chi == 0 ? 1.0 : -1.0;
-    for (int r = 0; r < 6; r++)
-      for (int c = r; c < 6; c++) bl.m[r][c] = factor * (p.m[r][c] + sg * q.m[r][c]);
-    for (int r = 0; r < 6; r++) bl.m[r][r] = mkc(bl.m[r][r].x + 1.0, 0.0);
-    block_inv(bl, A, AI, B, g.stride, i, chi);
+// The clover term in two passes over chunks of sites of one parity, so that
+// no thread holds both the six field strengths and a 6x6 block inversion:
+// k_clover_fields computes f(mu,nu) of one plane per thread (links loaded
+// where they are used, triple products by rows), k_clover_blocks builds one
+// chiral block per thread from the six planes and inverts it.  The
+// arithmetic of every entry is that of clover_f_mu_nu, init1/init2 and
+// block_inv above.
+
+// clover_f_mu_nu for the plane (MU, NU) with the loads of each leaf placed at
+// their use; the same products and sums as clover_f_mu_nu
+template <int MU, int NU>
+__device__ __forceinline__ void clover_f_plane(const Geom& g, const double2* gauge, L64& f, const int xs[4]) {
+  L64 t, r, c, d;
+  lzero(f);
+  {  // uuuu1: u1 u2 u3^+ u4^+
+    int xp_[4], x_p[4];
+    shift(g, xs, MU, 1, xp_);
+    shift(g, xs, NU, 1, x_p);
+    load_link(g, gauge, MU, xs, c); load_link(g, gauge, NU, xp_, d); mul2(t, c, false, d, false);
+    load_link(g, gauge, MU, x_p, c); load_link(g, gauge, NU, xs, d); mul3_rows(r, t, false, c, true, d, true);
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
   }
+  {  // uuuu2: u1 u2^+ u3^+ u4
+    int xm_[4], xmp[4];
+    shift(g, xs, MU, -1, xm_);
+    shift(g, xm_, NU, 1, xmp);
+    load_link(g, gauge, NU, xs, c); load_link(g, gauge, MU, xmp, d); mul2(t, c, false, d, true);
+    load_link(g, gauge, NU, xm_, c); load_link(g, gauge, MU, xm_, d); mul3_rows(r, t, false, c, true, d, false);
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  }
+  {  // uuuu3: u1^+ u2^+ u3 u4
+    int xm_[4], xmm[4], x_m[4];
+    shift(g, xs, MU, -1, xm_);
+    shift(g, xm_, NU, -1, xmm);
+    shift(g, xs, NU, -1, x_m);
+    load_link(g, gauge, MU, xm_, c); load_link(g, gauge, NU, xmm, d); mul2(t, c, true, d, true);
+    load_link(g, gauge, MU, xmm, c); load_link(g, gauge, NU, x_m, d); mul3_rows(r, t, false, c, false, d, false);
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  }
+  {  // uuuu4: u1^+ u2 u3 u4^+
+    int x_m[4], xp_[4], xpm[4];
+    shift(g, xs, NU, -1, x_m);
+    shift(g, xs, MU, 1, xp_);
+    shift(g, xp_, NU, -1, xpm);
+    load_link(g, gauge, NU, x_m, c); load_link(g, gauge, MU, x_m, d); mul2(t, c, true, d, false);
+    load_link(g, gauge, NU, xpm, c); load_link(g, gauge, MU, xs, d); mul3_rows(r, t, false, c, false, d, true);
+#pragma unroll
+    for (int p = 0; p < 3; p++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) f.m[p][q] = f.m[p][q] + r.m[p][q];
+  }
+  // clover_f_mu_nu.F90:92-102
+  C64 f10 = f.m[1][0], f20 = f.m[2][0], f21 = f.m[2][1];
+  f.m[0][0] = mkc(2.0 * f.m[0][0].y, 0.0);
+  f.m[1][1] = mkc(2.0 * f.m[1][1].y, 0.0);
+  f.m[2][2] = mkc(2.0 * f.m[2][2].y, 0.0);
+  f.m[0][1] = itimes(conjg(f10) - f.m[0][1]);
+  f.m[0][2] = itimes(conjg(f20) - f.m[0][2]);
+  f.m[1][2] = itimes(conjg(f21) - f.m[1][2]);
+  f.m[1][0] = conjg(f.m[0][1]);
+  f.m[2][0] = conjg(f.m[0][2]);
+  f.m[2][1] = conjg(f.m[1][2]);
 }
 
+// the planes of clover_init.F90:52-77 in the order used below:
+// 0 (1,0) and 1 (2,1), 2 (2,0) build p; 3 (2,3) and 4 (0,3), 5 (3,1) build q
+__global__ void __launch_bounds__(64) k_clover_fields(Geom g, const double2* gauge, int eo, int i0, int n,
+                                                      double2* tmp) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pl = blockIdx.y;
+  if (k >= n) return;
+  const Site st = site_coords(g, i0 + k, eo);
+  L64 f;
+  switch (pl) {
+    case 0: clover_f_plane<1, 0>(g, gauge, f, st.x); break;
+    case 1: clover_f_plane<2, 1>(g, gauge, f, st.x); break;
+    case 2: clover_f_plane<2, 0>(g, gauge, f, st.x); break;
+    case 3: clover_f_plane<2, 3>(g, gauge, f, st.x); break;
+    case 4: clover_f_plane<0, 3>(g, gauge, f, st.x); break;
+    default: clover_f_plane<3, 1>(g, gauge, f, st.x); break;
+  }
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) tmp[(size_t)(pl * 9 + r * 3 + c) * n + k] = make_double2(f.m[r][c].x, f.m[r][c].y);
+}
+
+__device__ __forceinline__ void load_plane(const double2* tmp, int n, int k, int pl, L64& f) {
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double2 v = tmp[(size_t)(pl * 9 + r * 3 + c) * n + k];
+      f.m[r][c] = mkc(v.x, v.y);
+    }
+}
+
+// clover_init3 (a1 = s(p+q)+1, a2 = s(p-q)+1, upper triangle) and
+// clover_inv for chiral block chi = blockIdx.y of each site
+__global__ void __launch_bounds__(64) k_clover_blocks(Geom g, const double2* tmp, int i0, int n, double factor,
+                                                      double2* A, double2* AI, double2* B) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int chi = blockIdx.y;
+  if (k >= n) return;
+  Blk p, q, bl;
+  L64 f, f2;
+  load_plane(tmp, n, k, 0, f);
+  init1(p, f);
+  load_plane(tmp, n, k, 1, f);
+  load_plane(tmp, n, k, 2, f2);
+  init2(p, f, f2);
+  load_plane(tmp, n, k, 3, f);
+  init1(q, f);
+  load_plane(tmp, n, k, 4, f);
+  load_plane(tmp, n, k, 5, f2);
+  init2(q, f, f2);
+  const double sg = chi == 0 ? 1.0 : -1.0;
+  for (int r = 0; r < 6; r++)
+    for (int c = r; c < 6; c++) bl.m[r][c] = factor * (p.m[r][c] + sg * q.m[r][c]);
+  for (int r = 0; r < 6; r++) bl.m[r][r] = mkc(bl.m[r][r].x + 1.0, 0.0);
+  block_inv(bl, A, AI, B, g.stride, i0 + k, chi);
+}
+
+int clover_init_chunk(const Geom& g) { return g.volh < (1 << 20) ? g.volh : (1 << 20); }
+
 void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, double2* a[2], double2* ainv[2],
-                        double2* b[2], cudaStream_t s) {
-  dim3 grid((g.volh + 63) / 64, 2);
-  k_clover_init<<<grid, 64, 0, s>>>(g, gauge, -csw_kappa / 8.0, a[0], a[1], ainv[0], ainv[1], b[0], b[1]);
+                        double2* b[2], double2* tmp, cudaStream_t s) {
+  const int chunk = clover_init_chunk(g);
+  for (int eo = 0; eo < 2; eo++) {
+    if (!a[eo] && !ainv[eo] && !b[eo]) continue;  // nothing wanted of this parity
+    for (int i0 = 0; i0 < g.volh; i0 += chunk) {
+      const int n = g.volh - i0 < chunk ? g.volh - i0 : chunk;
+      k_clover_fields<<<dim3((n + 63) / 64, 6), 64, 0, s>>>(g, gauge, eo, i0, n, tmp);
+      k_clover_blocks<<<dim3((n + 63) / 64, 2), 64, 0, s>>>(g, tmp, i0, n, -csw_kappa / 8.0, a[eo], ainv[eo],
+                                                            b[eo]);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kBlock) k_clover_action(Geom g, const double2* b, RedScratch red, double* out) {

@@ -67,6 +67,7 @@ struct bqcdg_ctx {
   double* mom_old = nullptr;     // their snapshot for the force monitor
   double2* gauge_bck = nullptr;  // saved links (restored on a rejected trajectory)
   double2* wbuf = nullptr;       // 6 planes x 9 complex per site
+  double2* clov_tmp = nullptr;   // field strengths of one chunk of clover_init
 
   std::map<int, double2*> fields;
   int next_handle = 1;

@@ -221,28 +221,6 @@ __device__ __forceinline__ void load_w(const Geom& g, const double2* w, int pl, 
     }
 }
 
-// r = op(a) op(b) op(c), one row of op(a) op(b) at a time: the same
-// products and sums as mul3, with a 3-element temporary instead of a matrix
-__device__ __forceinline__ void mul3_rows(L64& r, const L64& a, bool da, const L64& b, bool db, const L64& c,
-                                          bool dc) {
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    C64 t[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      C64 x = el(a, i, 0, da) * el(b, 0, k, db);
-      x = x + el(a, i, 1, da) * el(b, 1, k, db);
-      t[k] = x + el(a, i, 2, da) * el(b, 2, k, db);
-    }
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      C64 x = t[0] * el(c, 0, j, dc);
-      x = x + t[1] * el(c, 1, j, dc);
-      r.m[i][j] = x + t[2] * el(c, 2, j, dc);
-    }
-  }
-}
-
 // The two loops of clover_d_loop for one link and one plane.  Every link and
 // w matrix is loaded where it is used (the matrices are 36 registers each in
 // FP64; loaded together they spilled), so at most the two partial products,

@@ -172,9 +172,12 @@ void launch_clover_d(const Geom& g, double* p, const double2* gauge, const doubl
                      cudaStream_t st);
 
 // ---- clover construction (clover_init.cu) ----
-// clover_init.F90 + clover_inv.F90 on device: A, Ainv, B for both parities
+// clover_init.F90 + clover_inv.F90 on device: A, Ainv, B of each parity whose
+// pointers are given (null: not computed), in chunks of clover_init_chunk(g)
+// sites through tmp (54 complex per chunk site: the six field strengths)
+int clover_init_chunk(const Geom& g);
 void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, double2* a[2], double2* ainv[2],
-                        double2* b[2], cudaStream_t s);
+                        double2* b[2], double2* tmp, cudaStream_t s);
 // 2 sum log det over the halved 1/D of B (clover_action.F90)
 void launch_clover_action(const Geom& g, const double2* b, RedScratch red, double* out, cudaStream_t s);
 

@@ -36,6 +36,27 @@ __device__ __forceinline__ void mul3(L64& r, const L64& a, bool da, const L64& b
   mul2(t, a, da, b, db);
   mul2(r, t, false, c, dc);
 }
+// r = op(a) op(b) op(c), one row of op(a) op(b) at a time: the same
+// products and sums as mul3, with a 3-element temporary instead of a matrix
+__device__ __forceinline__ void mul3_rows(L64& r, const L64& a, bool da, const L64& b, bool db, const L64& c,
+                                          bool dc) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    C64 t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      C64 x = el(a, i, 0, da) * el(b, 0, k, db);
+      x = x + el(a, i, 1, da) * el(b, 1, k, db);
+      t[k] = x + el(a, i, 2, da) * el(b, 2, k, db);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      C64 x = t[0] * el(c, 0, j, dc);
+      x = x + t[1] * el(c, 1, j, dc);
+      r.m[i][j] = x + t[2] * el(c, 2, j, dc);
+    }
+  }
+}
 // su3.F90:196-214: p_j += s Im Tr(lambda_j v)
 __device__ __forceinline__ void im_tr_j(double p[8], const L64& v, double s) {
   p[0] += s * (v.m[0][1].y + v.m[1][0].y);
