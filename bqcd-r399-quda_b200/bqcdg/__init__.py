@@ -95,6 +95,7 @@ def _lib_handle():
         L.bqcdg_get_gauge.argtypes = [vp, dp, i]
         L.bqcdg_load_clover.argtypes = [vp, dp, dp, dp]
         L.bqcdg_get_clover.argtypes = [vp, dp, dp, dp]
+        L.bqcdg_load_clover_solver.argtypes = [vp, dp, dp]
         L.bqcdg_clover_init.argtypes = [vp, C.c_double]
         L.bqcdg_clover_init_solver.argtypes = [vp, C.c_double]
         L.bqcdg_release_scratch.argtypes = [vp, i]
@@ -273,6 +274,12 @@ class Lattice:
         """clover_init keeping only the two parts the even-odd solver uses (A
         even, A^-1 odd): a third of the clover memory of clover_init."""
         _check(lib().bqcdg_clover_init_solver(self.h, csw_kappa), "clover_init_solver")
+
+    def load_clover_solver(self, a, ainv):
+        """load_clover keeping only what the even-odd solver reads: A of the
+        even sites and A^-1 of the odd ones, from the full arrays."""
+        _check(lib().bqcdg_load_clover_solver(self.h, _ptr(a, np.complex128), _ptr(ainv, np.complex128)),
+               "load_clover_solver")
 
     def get_clover(self):
         out = [np.zeros((2, self.volh, 2, 18), np.complex128) for _ in range(3)]

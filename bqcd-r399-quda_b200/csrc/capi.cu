@@ -806,8 +806,10 @@ int bqcdg_get_gauge(bqcdg_ctx* c, double* u, int flipped) {
   return BQCDG_OK;
 }
 
-static int load_clover_field(bqcdg_ctx* c, double2** dst, bool* have, const double* src) {
-  for (int eo = 0; eo < 2; eo++) {
+// the parities eo0..eo1 of one clover field from its Fortran array
+static int load_clover_field(bqcdg_ctx* c, double2** dst, bool* have, const double* src, int eo0 = 0,
+                             int eo1 = 1) {
+  for (int eo = eo0; eo <= eo1; eo++) {
     if (!dst[eo]) CK(c->alloc((void**)&dst[eo], (size_t)36 * c->g.stride * sizeof(double2)));
     size_t n = (size_t)c->g.volh * 36 * sizeof(double2);
     CK(c->stage(n));
@@ -835,6 +837,26 @@ int bqcdg_load_clover(bqcdg_ctx* c, const double* a, const double* ainv, const d
       c->have_Ainv[eo] = true;
     }
   }
+  for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+
+int bqcdg_load_clover_solver(bqcdg_ctx* c, const double* a, const double* ainv) {
+  if (!c || !a || !ainv) return BQCDG_EINVAL;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  // only A of the even sites and A^-1 of the odd ones; the parts the even-odd
+  // operator does not read are released
+  double2** unused[4] = {&c->A[1], &c->Ainv[0], &c->B[0], &c->B[1]};
+  for (double2** f : unused) {
+    c->release(*f);
+    *f = nullptr;
+  }
+  c->have_A[1] = c->have_Ainv[0] = c->have_B[0] = c->have_B[1] = false;
+  int st;
+  if ((st = load_clover_field(c, c->A, c->have_A, a, 0, 0))) return st;
+  if ((st = load_clover_field(c, c->Ainv, c->have_Ainv, ainv, 1, 1))) return st;
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
   CK(cudaStreamSynchronize(c->stream));
   return BQCDG_OK;

@@ -127,6 +127,11 @@ int bqcdg_get_gauge(bqcdg_ctx *ctx, double *u, int flipped);
  * load_clover_quda (invert_quda.F90:138). */
 int bqcdg_load_clover(bqcdg_ctx *ctx, const double *a, const double *ainv, const double *b);
 int bqcdg_get_clover(bqcdg_ctx *ctx, double *a, double *ainv, double *b);
+/* load_clover for the solver only: from the same arrays, A of the even
+ * sites and A^-1 of the odd ones, the two parts M~ and W read; a third of
+ * the bytes of bqcdg_load_clover(a, ainv, b).  The other parts are released
+ * (entry points that need them then return BQCDG_ENOCLOVER). */
+int bqcdg_load_clover_solver(bqcdg_ctx *ctx, const double *a, const double *ainv);
 /* clover_init(a, i, b, u, csw_kappa) (clover/clover_init.F90:28) on the
  * device, from the loaded links */
 int bqcdg_clover_init(bqcdg_ctx *ctx, double csw_kappa);

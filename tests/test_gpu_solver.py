@@ -102,3 +102,22 @@ def test_relative_tolerance_1e10(setup, bq, prec):
     assert info.true_rtr <= 1e-20 * info.b2
     r = lat.mtdagmt(x, para) - b
     assert np.linalg.norm(r) <= 1.01e-10 * np.linalg.norm(b)
+
+
+def test_solver_only_clover_upload(setup, bq):
+    """load_clover_solver takes the same Fortran arrays and keeps A (even) and
+    A^-1 (odd) only: the solve is bit-identical to one with the full upload,
+    and the force-side parts report their absence."""
+    g, lat = setup["g"], setup["lat"]
+    para = bq.HmcPara(kappa=setup["kappa"], csw=setup["csw"], rho=0.1)
+    b = g.gauss_spinor(0)
+    x_full, info = lat.solve(np.zeros_like(b), b, para, precision=bq.PREC_DOUBLE, tol=1e-12)
+    a, ai, bb = setup["clov"]
+    lat.load_clover_solver(a, ai)
+    x_lean, info2 = lat.solve(np.zeros_like(b), b, para, precision=bq.PREC_DOUBLE, tol=1e-12)
+    assert info.converged and info2.converged
+    assert np.array_equal(x_full, x_lean)
+    with pytest.raises(bq.BqcdgError) as e:
+        lat.clover_action(1)
+    assert e.value.status == bq.ENOCLOVER
+    lat.load_clover(*setup["clov"])   # restore the full set for the other tests
