@@ -277,6 +277,7 @@ def run_ours(args):
         h2d = u_host.nbytes + a_host.nbytes // 2 + i_host.nbytes // 2 + b_host.nbytes + x_host.nbytes
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(x.nbytes),
                "converged": bool(einfo.converged)}
+        lat.clover_init(CSW * KAPPA)   # all six clover parts again (the lean upload kept two)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
