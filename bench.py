@@ -476,8 +476,9 @@ def run_batch(args):
     default workload's action; its gauge construction followed by the
     pure-gauge thermalisation of the hmc workload): the 12
     spin-colour point sources at the origin plus 4 Gaussian vectors, solved
-    to true |r|/|b| < 1e-10 as one batched block CG (FP32 iterations, FP64
-    reliable updates, autotuned right-hand sides per launch), against
+    to true |r|/|b| < 1e-10 as one batched CG: 16 independent CG recurrences
+    whose stencil passes share one launch (FP32 iterations, FP64 reliable
+    updates, autotuned right-hand sides per thread), against
     sequential single-RHS solves of the same systems.  The sequential time is
     one point-source and one Gaussian solve scaled to 12 + 4; both arms run
     the same precision and stopping rule."""
