@@ -154,6 +154,7 @@ def _lib_handle():
         L.bqcdg_cg_dev.argtypes = [vp, i, i, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
         L.bqcdg_field_cdot.argtypes = [vp, i, i, pd, pd]
         L.bqcdg_field_caxpby.argtypes = [vp, i, d, d, d, i]
+        L.bqcdg_field_cdot_pairs.argtypes = [vp, i, P(C.c_int), P(C.c_int), pd, pd]
         _LIB = L
     return _LIB
 
@@ -455,6 +456,23 @@ class Lattice:
         re, im = C.c_double(), C.c_double()
         _check(lib().bqcdg_field_cdot(self.h, ha, hb, C.byref(re), C.byref(im)), "field_cdot")
         return complex(re.value, im.value)
+
+    MAX_DOT_PAIRS = 8   # BQCDG_MAX_DOT_PAIRS
+
+    def field_cdot_pairs(self, pairs):
+        """[<a, b> for (a, b) in pairs] of resident fields, each equal to
+        field_cdot(a, b) bit for bit, in launches of up to MAX_DOT_PAIRS
+        pairs with one read-back each."""
+        out = []
+        for k in range(0, len(pairs), self.MAX_DOT_PAIRS):
+            chunk = pairs[k:k + self.MAX_DOT_PAIRS]
+            n = len(chunk)
+            ha = (C.c_int * n)(*[a for a, _ in chunk])
+            hb = (C.c_int * n)(*[b for _, b in chunk])
+            re, im = (C.c_double * n)(), (C.c_double * n)()
+            _check(lib().bqcdg_field_cdot_pairs(self.h, n, ha, hb, re, im), "field_cdot_pairs")
+            out.extend(complex(re[j], im[j]) for j in range(n))
+        return out
 
     def field_caxpby(self, hy, ay, a, hx):
         """y = ay y + a x (a complex) on resident fields."""

@@ -49,15 +49,18 @@ class Mre:
         self.rank = min(self.rank + 1, self.nvec)
 
     def _gram_schmidt(self):
-        """mre.F90:189-213 (real scalar products)."""
+        """mre.F90:189-213 (real scalar products).  The products of the
+        normalised v_k with the later vectors do not depend on one another,
+        so each step reads them back in one call."""
         lat = self.lat
         for k in range(self.rank):
             vk = self.vec[k]
             rkk = lat.field_cdot(vk, vk).real
             lat.field_caxpby(vk, 0.0, 1.0 / math.sqrt(rkk), vk)
-            for j in range(k + 1, self.rank):
-                rkj = lat.field_cdot(vk, self.vec[j]).real
-                lat.field_caxpby(self.vec[j], 1.0, -rkj, vk)
+            later = self.vec[k + 1:self.rank]
+            rk = lat.field_cdot_pairs([(vk, vj) for vj in later])
+            for vj, rkj in zip(later, rk):
+                lat.field_caxpby(vj, 1.0, -rkj.real, vk)
 
     @staticmethod
     def _gauss_jordan(a, b):
@@ -108,16 +111,18 @@ class Mre:
             return
         self._gram_schmidt()
         r = self.rank
-        bb = np.zeros(r, complex)
         for i in range(r):
-            bb[i] = lat.field_cdot(self.vec[i], phi)
             lat.op_dev(op, self.mv[i], self.vec[i], para, rho=rho)
+        bb = np.array(lat.field_cdot_pairs([(self.vec[i], phi) for i in range(r)]), complex)
+        upper = [(i, j) for i in range(r) for j in range(i, r)]
+        dots = lat.field_cdot_pairs([(self.mv[i], self.mv[j]) for i, j in upper])
         ga = np.zeros((r, r), complex)
-        for i in range(r):
-            ga[i, i] = lat.field_cdot(self.mv[i], self.mv[i]).real
-            for j in range(i + 1, r):
-                ga[i, j] = lat.field_cdot(self.mv[i], self.mv[j])
-                ga[j, i] = np.conj(ga[i, j])
+        for (i, j), v in zip(upper, dots):
+            if i == j:
+                ga[i, i] = v.real
+            else:
+                ga[i, j] = v
+                ga[j, i] = np.conj(v)
         x = self._gauss_jordan(ga, bb)
         lat.field_caxpby(trial, 0.0, x[0], self.vec[0])
         for i in range(1, r):

@@ -212,6 +212,27 @@ int bqcdg_field_cdot(bqcdg_ctx* c, int ha, int hb, double* re, double* im) {
   return BQCDG_OK;
 }
 
+int bqcdg_field_cdot_pairs(bqcdg_ctx* c, int n, const int* ha, const int* hb, double* re, double* im) {
+  if (!c || n < 1 || n > BQCDG_MAX_DOT_PAIRS || !ha || !hb || !re || !im) return BQCDG_EINVAL;
+  static_assert(BQCDG_MAX_DOT_PAIRS == kMaxDotPairs, "one limit for the header and the kernel");
+  FieldPairs fp{};
+  for (int j = 0; j < n; j++) {
+    fp.a[j] = field(c, ha[j]);
+    fp.b[j] = field(c, hb[j]);
+    if (!fp.a[j] || !fp.b[j]) return BQCDG_EINVAL;
+  }
+  CK(cudaSetDevice(c->device));
+  launch_cdot_pairs(c->g, fp, n, c->red, c->dres, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->hres, c->dres, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int j = 0; j < n; j++) {
+    re[j] = c->hres[2 * j];
+    im[j] = c->hres[2 * j + 1];
+  }
+  return BQCDG_OK;
+}
+
 int bqcdg_field_caxpby(bqcdg_ctx* c, int hy, double ay, double are, double aim, int hx) {
   if (!c || !field(c, hy) || !field(c, hx)) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));

@@ -255,6 +255,53 @@ void launch_cdot(const Geom& g, const double2* a, const double2* b, RedScratch r
   k_cdot<<<nblocks(g.volh), kBlock, 0, s>>>(g, a, b, red, out);
 }
 
+// out[2j] + i out[2j+1] = <a_j, b_j> for j < NB, in one pass: each product
+// and each sum is k_cdot's, in k_cdot's order (the per-value block
+// reduction does not depend on NB), so every result equals k_cdot's bit for
+// bit.  MRE (mre.F90:68-213) needs up to nvec(nvec+1)/2 of them at a time.
+template <int NB>
+__global__ void __launch_bounds__(kBlock) k_cdot_pairs(Geom g, FieldPairs fp, RedScratch red, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[2 * NB];
+#pragma unroll
+  for (int j = 0; j < 2 * NB; j++) acc[j] = 0.0;
+  if (i < g.volh) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+#pragma unroll
+      for (int j = 0; j < NB; j++) {
+        const double2 x = fp.a[j][k * g.stride + i], y = fp.b[j][k * g.stride + i];
+        acc[2 * j] += x.x * y.x + x.y * y.y;
+        acc[2 * j + 1] += x.x * y.y - x.y * y.x;
+      }
+    }
+  }
+  block_reduce_store<2 * NB>(acc, red.partial, red.maxblocks, blockIdx.x);
+  if (last_block(red.counter, gridDim.x)) {
+    double tot[2 * NB];
+    final_sum<2 * NB>(red.partial, red.maxblocks, gridDim.x, tot);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int j = 0; j < 2 * NB; j++) out[j] = tot[j];
+      *red.counter = 0;
+    }
+  }
+}
+
+void launch_cdot_pairs(const Geom& g, const FieldPairs& fp, int n, RedScratch red, double* out, cudaStream_t s) {
+  const int nb = nblocks(g.volh);
+  switch (n) {
+    case 1: k_cdot_pairs<1><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 2: k_cdot_pairs<2><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 3: k_cdot_pairs<3><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 4: k_cdot_pairs<4><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 5: k_cdot_pairs<5><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 6: k_cdot_pairs<6><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    case 7: k_cdot_pairs<7><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+    default: k_cdot_pairs<8><<<nb, kBlock, 0, s>>>(g, fp, red, out); break;
+  }
+}
+
 // y = ay y + a x with complex a (ay real: 1 for an axpy, 0 to overwrite y)
 __global__ void __launch_bounds__(kBlock) k_caxpby(Geom g, double are, double aim, const double2* x, double ay,
                                                    double2* y) {

@@ -200,6 +200,13 @@ void launch_dsg(const Geom& g, const double2* gauge, double* p, double s, cudaSt
 void launch_mom_sumsq(const Geom& g, const double* a, const double* b, RedScratch red, double* out, cudaStream_t s);
 // out[0] + i out[1] = <a, b> of F64 spinors
 void launch_cdot(const Geom& g, const double2* a, const double2* b, RedScratch red, double* out, cudaStream_t s);
+// up to kMaxDotPairs field pairs (a_j, b_j) whose <a_j, b_j> one launch computes
+constexpr int kMaxDotPairs = 8;
+struct FieldPairs {
+  const double2* a[kMaxDotPairs];
+  const double2* b[kMaxDotPairs];
+};
+void launch_cdot_pairs(const Geom& g, const FieldPairs& fp, int n, RedScratch red, double* out, cudaStream_t s);
 // y = ay y + (are + i aim) x
 void launch_caxpby(const Geom& g, double are, double aim, const double2* x, double ay, double2* y, cudaStream_t s);
 

@@ -321,6 +321,12 @@ int bqcdg_cg_dev(bqcdg_ctx *ctx, int hx, int hb, const bqcdg_params *p, const bq
  * complex a (the linear combinations of mre.F90:68-213) on resident fields */
 int bqcdg_field_cdot(bqcdg_ctx *ctx, int ha, int hb, double *re, double *im);
 int bqcdg_field_caxpby(bqcdg_ctx *ctx, int hy, double ay, double are, double aim, int hx);
+/* re[j] + i im[j] = <ha[j], hb[j]> for j < n <= BQCDG_MAX_DOT_PAIRS, in one
+ * pass and one read-back: each value equals bqcdg_field_cdot's bit for bit.
+ * The scalar products of one mre.F90 step (Gram-Schmidt, mre.F90:189-213,
+ * and the Gram system, mre.F90:68-146) come in a few such calls. */
+#define BQCDG_MAX_DOT_PAIRS 8
+int bqcdg_field_cdot_pairs(bqcdg_ctx *ctx, int n, const int *ha, const int *hb, double *re, double *im);
 
 /* ---- allocation-free operator ------------------------------------------- */
 /* This entry point has no counterpart in the reference.  It is for callers

@@ -99,6 +99,13 @@ def test_resident_forces_and_ops_match_host_entry_points(oracle, bq, pair):
     lat.field_caxpby(hc, 0.5, 0.25 - 2j, ha)
     ref = 0.5 * lat.w_dagger_w(a, para) + (0.25 - 2j) * a
     assert np.linalg.norm(lat.field_get(hc) - ref) <= 1e-14 * np.linalg.norm(ref)
+    # the batched products of the MRE guess: each equal to field_cdot's bit
+    # for bit, in launches of 1 to 8 pairs (ragged last launch of 11 pairs)
+    hs = [ha, hb, hc, lat.field(g.gauss_spinor(0))]
+    pairs = [(hs[i % 4], hs[(3 * i + 1) % 4]) for i in range(11)]
+    for n in (1, 2, 5, 8, 11):
+        got = lat.field_cdot_pairs(pairs[:n])
+        assert got == [lat.field_cdot(x, y) for x, y in pairs[:n]]
 
 
 def test_resident_cg_matches_reference_cg(oracle, bq, pair):
