@@ -55,6 +55,10 @@ def test_error_strings_and_argument_checks(so):
     assert lib.bqcdg_create(None, L, bc, 0) == 1
     assert lib.bqcdg_destroy(None) == 1
     assert lib.bqcdg_d(None, 0, 1, None, None) == 1
+    ha, hb = (C.c_int * 9)(*range(9)), (C.c_int * 9)(*range(9))
+    re_, im_ = (C.c_double * 9)(), (C.c_double * 9)()
+    assert lib.bqcdg_field_cdot_pairs(None, 2, ha, hb, re_, im_) == 1
+    assert lib.bqcdg_field_cdot_pairs(None, 9, ha, hb, re_, im_) == 1   # more than BQCDG_MAX_DOT_PAIRS
 
 
 def test_no_device_is_reported_not_faulted(so):
