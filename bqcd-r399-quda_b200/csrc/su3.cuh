@@ -98,20 +98,25 @@ __device__ __forceinline__ void load_link(const Geom& g, const double2* gauge, i
   U.load(mu, parity_of(x), site_index(g, x), u);
 }
 
-// staple.F90:28-63: sum over nu != mu of the forward and backward staples
-__device__ __forceinline__ void staple(const Geom& g, const double2* gauge, const int x[4], int mu, L64& st) {
+// staple.F90:28-63: sum over nu != mu of the forward and backward staples.
+// With mu a template parameter every shifted coordinate is a register (a
+// run-time mu indexes the coordinate arrays, which puts them in local
+// memory); staple() dispatches on a run-time mu, uniform across a launch.
+template <int MU>
+__device__ __forceinline__ void staple_t(const Geom& g, const double2* gauge, const int x[4], L64& st) {
   lzero(st);
+#pragma unroll
   for (int nu = 0; nu < 4; nu++) {
-    if (nu == mu) continue;
+    if (nu == MU) continue;
     int x1[4], x2[4], x3[4], x4[4];
-    shift(g, x, mu, 1, x1);
+    shift(g, x, MU, 1, x1);
     shift(g, x, nu, 1, x2);
     shift(g, x, nu, -1, x3);
-    shift(g, x3, mu, 1, x4);
+    shift(g, x3, MU, 1, x4);
     L64 a, b, c, t, r;
     // uuu_fwd: U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
     load_link(g, gauge, nu, x1, a);
-    load_link(g, gauge, mu, x2, b);
+    load_link(g, gauge, MU, x2, b);
     load_link(g, gauge, nu, x, c);
     mul2(t, a, false, b, true);
     mul2(r, t, false, c, true);
@@ -119,12 +124,20 @@ __device__ __forceinline__ void staple(const Geom& g, const double2* gauge, cons
       for (int q = 0; q < 3; q++) st.m[p][q] = st.m[p][q] + r.m[p][q];
     // uuu_bwd: U_nu(x-nu+mu)^+ U_mu(x-nu)^+ U_nu(x-nu)
     load_link(g, gauge, nu, x4, a);
-    load_link(g, gauge, mu, x3, b);
+    load_link(g, gauge, MU, x3, b);
     load_link(g, gauge, nu, x3, c);
     mul2(t, a, true, b, true);
     mul2(r, t, false, c, false);
     for (int p = 0; p < 3; p++)
       for (int q = 0; q < 3; q++) st.m[p][q] = st.m[p][q] + r.m[p][q];
+  }
+}
+__device__ __forceinline__ void staple(const Geom& g, const double2* gauge, const int x[4], int mu, L64& st) {
+  switch (mu) {
+    case 0: staple_t<0>(g, gauge, x, st); break;
+    case 1: staple_t<1>(g, gauge, x, st); break;
+    case 2: staple_t<2>(g, gauge, x, st); break;
+    default: staple_t<3>(g, gauge, x, st); break;
   }
 }
 
