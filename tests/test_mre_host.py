@@ -112,3 +112,28 @@ def test_rank_one_and_reset():
     assert np.array_equal(lat.f[trial_h], lat.f[h])
     mre.put(h, True)
     assert mre.rank == 0
+
+
+def test_lattice_wrapper_splits_pairs_into_launches(bq, monkeypatch):
+    """Lattice.field_cdot_pairs against a stand-in for the library call: at
+    most MAX_DOT_PAIRS pairs per call, in order, results in order."""
+    calls = []
+
+    class FakeLib:
+        def bqcdg_field_cdot_pairs(self, h, n, ha, hb, re, im):
+            calls.append((h, n, list(ha)[:n], list(hb)[:n]))
+            for j in range(n):
+                re[j] = 10.0 * ha[j] + hb[j]
+                im[j] = -float(ha[j])
+            return 0
+
+    monkeypatch.setattr(bq, "lib", lambda: FakeLib())
+    lat = object.__new__(bq.Lattice)
+    lat.h = "ctx"
+    pairs = [(a, a + 1) for a in range(11)]
+    got = lat.field_cdot_pairs(pairs)
+    assert [c[1] for c in calls] == [8, 3] and all(c[0] == "ctx" for c in calls)
+    assert [c[2] for c in calls] == [list(range(8)), [8, 9, 10]]
+    assert got == [complex(10.0 * a + a + 1, -a) for a in range(11)]
+    calls.clear()
+    assert lat.field_cdot_pairs([]) == [] and not calls
