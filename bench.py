@@ -124,7 +124,7 @@ def dist_init():
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl" if _has_cuda() else "gloo", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl" if _has_cuda() else "gloo", timeout=datetime.timedelta(seconds=300),
                                 device_id=None)
         pg = dist
     return world, rank, local, pg
@@ -196,12 +196,15 @@ def build_system(bq, L, device, seed_skip, cool):
 TRAFFIC_PER_SITE_INT16 = 437.6
 
 
-def stencil_bytes_per_site(prec):
+def stencil_bytes_per_site(prec, rec12=True):
     """Algorithmic bytes of one mtil first-half pass (D_oe + Ainv_oo) per odd
     output site: read the input spinor once, 8 links, one clover block, write
-    one spinor.  int16 fields carry one 4-byte norm per spinor/clover site."""
+    one spinor.  int16 fields carry one 4-byte norm per spinor/clover site.
+    FP64 links are read as 12 reals (96 B) when the context holds SU(3)
+    links, as every benchmark system here does (the device generators keep
+    them unitary), else as 18 reals (144 B)."""
     if prec == 0:
-        s, gl, c = 192, 144, 576          # FP64, 18-real links
+        s, gl, c = 192, (96 if rec12 else 144), 576
     elif prec == 1:
         s, gl, c = 96, 48, 288            # FP32, 12-real links
     else:
@@ -251,7 +254,7 @@ def run_ours(args):
     st_bytes = stencil_bytes_per_site(2) * lat.volh
     st_gbs = st_bytes / (st_ms * 1e-3) / 1e9
     f64_ms = sum(i.stencil_ms for i in fp64) / max(1, sum(i.stencil_launches for i in fp64))
-    f64_gbs = stencil_bytes_per_site(0) * lat.volh / (f64_ms * 1e-3) / 1e9
+    f64_gbs = stencil_bytes_per_site(0, rec12=True) * lat.volh / (f64_ms * 1e-3) / 1e9
 
     # e2e through the reference-facing call (host arrays, transfers timed)
     e2e = None
@@ -272,16 +275,23 @@ def run_ours(args):
         a_host, i_host = (pinned(c) for c in lat.get_clover()[:2])
         b_host = pinned(lat.field_get(hb))
         x_host = pinned(np.zeros_like(b_host))
-        lat2 = lat
-        barrier(pg, local)
-        t0 = time.perf_counter()
-        lat2.load_gauge(u_host, flipped=True)
-        lat2.load_clover_solver(a_host, i_host)      # A even and A^-1 odd: what the solver reads
-        x, einfo = lat2.solve(x_host, b_host, para, precision=bq.PREC_HALF, tol=args.tol, inplace=True)
-        e2e_s = allmax(pg, time.perf_counter() - t0, local)
+        e2e_t, e2e_ok = [], True
+        n_e2e = args.e2e_steps if args.e2e_steps > 0 else args.steps
+        for k in range(1 + n_e2e):           # one untimed call, then the timed ones
+            x_host[...] = 0.0
+            barrier(pg, local)
+            t0 = time.perf_counter()
+            lat.load_gauge(u_host, flipped=True)
+            lat.load_clover_solver(a_host, i_host)      # A even and A^-1 odd: what the solver reads
+            x, einfo = lat.solve(x_host, b_host, para, precision=bq.PREC_HALF, tol=args.tol, inplace=True)
+            dt = time.perf_counter() - t0
+            if k > 0:
+                e2e_t.append(allmax(pg, dt, local))
+                e2e_ok = e2e_ok and bool(einfo.converged)
         h2d = u_host.nbytes + a_host.nbytes // 2 + i_host.nbytes // 2 + b_host.nbytes + x_host.nbytes
-        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(x.nbytes),
-               "converged": bool(einfo.converged)}
+        e2e = {"value": sum(e2e_t) / len(e2e_t), "unit": "s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(x.nbytes), "converged": e2e_ok, "steps": len(e2e_t),
+               "min_s": min(e2e_t), "max_s": max(e2e_t)}
         lat.clover_init(CSW * KAPPA)   # all six clover parts again (the lean upload kept two)
 
     cpu = None
@@ -306,17 +316,16 @@ def run_ours(args):
             "dtype": "f64 (int16/f32 sloppy iterations)",
             "data": "synthetic: device hot start (BQCD ranf, default seed) + %d conf_relax cooling sweep(s) "
                     "(plaquette %.4f), Gaussian b" % (lat.sweeps, plaq),
-            "config": {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
-                                   % ("x".join(map(str, L)), KAPPA, CSW),
-                       "lattice": list(L), "volh": lat.volh, "plaquette": round(plaq, 6),
-                       "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 (no flush)"},
+            "config": solve_config(L, lat.sweeps, plaq, lat.volh, world),
             "mixed": {"time_s": step_s, "iterations": it.niter, "reliable_updates": it.reliable_updates,
                       "true_rel_residual": (it.true_rtr / it.b2) ** 0.5, "converged": ok,
                       "gflops": round(gflops, 1), "wall_s_per_step": wall / args.steps},
-            "fp64": {"time_s": fp64_s, "iterations": fp64[0].niter,
+            "fp64": {"time_s": fp64_s, "steps": len(fp64), "iterations": fp64[0].niter,
                      "true_rel_residual": (fp64[0].true_rtr / fp64[0].b2) ** 0.5,
                      "dslash_gbs": round(f64_gbs, 1), "dslash_frac": round(f64_gbs / peak, 4),
-                     "dslash_frac_nominal": round(f64_gbs / NOMINAL_HBM_GBS, 4)},
+                     "dslash_frac_nominal": round(f64_gbs / NOMINAL_HBM_GBS, 4),
+                     "dslash_bytes_per_site": stencil_bytes_per_site(0, rec12=True),
+                     "dslash_kernel": "k_pass1<F64> (12-real SU(3) links)"},
             "speedup_mixed_vs_fp64": round(fp64_s / step_s, 3),
             "roofline": {"bound": "hbm", "achieved": round(st_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(st_gbs / peak, 4), "traffic": int(TRAFFIC_PER_SITE_INT16 * lat.volh),
@@ -359,8 +368,24 @@ def cpu_baseline(lat, hb, L, fp64_iters, seconds):
                       "iterations of the FP64 GPU CG" % (n, "x".join(map(str, L)), dt, per_iter, fp64_iters)}
 
 
+def solve_config(L, sweeps, plaq, volh, world):
+    """The config object of the default line, shared by both arms."""
+    return {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
+                        % ("x".join(map(str, L)), KAPPA, CSW),
+            "lattice": list(L), "volh": volh, "sweeps": sweeps, "plaquette": round(plaq, 6),
+            "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 (no flush)"}
+
+
 def run_reference(args):
-    """CPU restatement of the reference's CG path on the host cores."""
+    """The reference's CG path on the host cores: the oracle's FP64 CG (a C
+    restatement of cg.F90 over mtdagmt and the D21/clover routines, OpenMP on
+    all host threads) on the same system as the GPU arm, built on the host by
+    the same generators.  One full solve from x = 0 to |r|/|b| < 1e-10 is
+    timed, and its true residual recomputed with the oracle's operator: that
+    solve is the line's value.  The K timed steps (after W warm-up ones) are
+    bounded samples of the same CG, each a fixed number of iterations scaled
+    to the measured iteration count; they are reported beside the value as
+    a check of its per-iteration cost.  Under torchrun only rank 0 works."""
     import numpy as np
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -371,56 +396,58 @@ def run_reference(args):
     g = O.Geom(L, (1, 1, 1, -1))
     O.ranset(0)
     u = g.hot()
+    sweeps = 0
     if args.cool >= 0:
         g.relax(u, args.cool)
+        sweeps = args.cool
     else:
-        sweeps = 0
         while sweeps < COOL and 1.0 - g.sg(u) / (6.0 * 2 * g.volh) < PLAQ_TARGET:
             g.relax(u, 1)
             sweeps += 1
+    plaq = 1.0 - g.sg(u) / (6.0 * 2 * g.volh)
     clov = g.clover_init(u, CSW * KAPPA)
     g.flip_bc(u)
     O.ranset(0)
     b = g.gauss_spinor(0, 0.5)
-    # iterations to 1e-10 of the same FP64 algorithm: one CPU solve within a
-    # time budget; if the budget ends first, the count is extrapolated from
-    # the residual decay rate of the iterations that ran
-    import math
     b2 = float(np.vdot(b, b).real)
-    rest = np.float32(1e-20 * b2)
+    # the stopping rule of the GPU arm: |r|^2 <= tol^2 |b|^2 on the iterated
+    # residual (cg.F90:111 with rest = tol^2 |b|^2), then the true residual
+    rest = np.float32(args.tol ** 2 * b2)
     t0 = time.perf_counter()
-    g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=0.0, maxiter=2, log=2)
-    per_iter = (time.perf_counter() - t0) / 2
-    cap = max(4, min(args.ref_maxiter, int(args.ref_budget / max(per_iter, 1e-9))))
-    t0 = time.perf_counter()
-    _, iters, rtr, _ = g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=rest,
-                            maxiter=cap, log=2)
+    x, iters, rtr, rc = g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=rest,
+                             maxiter=args.ref_maxiter, log=2)
     full = time.perf_counter() - t0
-    per_iter = full / max(1, iters)
-    exact = rtr <= rest
-    if not exact:
-        rate = math.log(rtr / b2) / iters
-        iters = int(math.ceil(math.log(1e-20) / rate))
-    steps = []
+    ax = g.op("mtdagmt", x, u, clov, KAPPA, CSW * KAPPA)
+    true_rel = float(np.linalg.norm(b - ax) / np.sqrt(b2))
+    converged = rtr <= rest
+    per_iter_full = full / max(1, iters)
+    n = max(10, min(iters, int(args.ref_sample_seconds / max(per_iter_full, 1e-9))))
+    samples = []
     for k in range(args.warmup + args.steps):
-        n = max(2, min(iters, int(args.cpu_seconds / max(per_iter, 1e-9))))
         t0 = time.perf_counter()
         g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, 0.0, 0.0, rest=0.0, maxiter=n, log=2)
         dt = time.perf_counter() - t0
         if k >= args.warmup:
-            steps.append(dt / n * iters)
-    v = sum(steps) / len(steps)
-    out = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64", "data": "synthetic (same generators on the host)", "impl": "reference",
-           "config": {"workload": "M^+M CG to true |r|/|b|<1e-10, lattice %s, kappa %.4f, c_sw %.4f, bc t -1"
-                                  % ("x".join(map(str, L)), KAPPA, CSW), "lattice": list(L)},
-           "cpu_baseline": {"value": v, "unit": "s", "cores": O.threads(), "kind": "port",
-                            "sample": "%s: %d iterations to 1e-10 (%.1f s of CPU solve); each step times a "
-                                      "bounded sample of iterations and scales to %d"
-                                      % ("full solve" if exact else "extrapolated from the residual decay of a "
-                                         "time-capped solve", iters, full, iters)},
-           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            samples.append(dt / n * iters)
+    cfg = solve_config(L, sweeps, plaq, g.volh, world)
+    out = {"metric": METRIC, "value": round(full, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(full * 1e3, 1), "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic: host hot start (BQCD ranf, default seed) + %d conf_relax cooling sweep(s) "
+                   "(plaquette %.4f), Gaussian b" % (sweeps, plaq),
+           "impl": "reference", "config": cfg,
+           "full_solve": {"seconds": round(full, 4), "iterations": iters, "converged": bool(converged),
+                          "iterated_rel_residual": float(np.sqrt(max(rtr, 0.0) / b2)),
+                          "true_rel_residual": true_rel, "s_per_iteration": per_iter_full},
+           "sampled_steps": {"iterations_per_sample": n, "scaled_s": [round(v, 3) for v in samples],
+                             "mean_scaled_s": round(sum(samples) / len(samples), 4)},
+           "cpu_baseline": {"value": round(full, 4), "unit": "s", "cores": O.threads(), "kind": "port",
+                            "sample": "one full FP64 CG solve (cg.F90 restated, M~^+M~ at %s) from x = 0: %d "
+                                      "iterations, true |r|/|b| %.2e, %.1f s; then %d timed samples of %d "
+                                      "iterations each, scaled to %d iterations (mean %.1f s)"
+                                      % ("x".join(map(str, L)), iters, true_rel, full, len(samples), n, iters,
+                                         sum(samples) / len(samples))},
+           "e2e": {"value": round(full, 4), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
@@ -847,6 +874,59 @@ def run_confio(args):
         pg.destroy_process_group()
 
 
+def run_plumbing(args):
+    """CPU stand-in for the replica plumbing of the other workloads, for
+    testing bench.py --gpus N without a GPU: every rank times the oracle's
+    M~^+M~ CG on its own seeded 4^4 system between the same barriers, the
+    step time is the max over ranks, and rank 0 prints one line with every
+    rank's time beside it.  Not a benchmark."""
+    import numpy as np
+    from oracle import oracle as O
+    world, rank, local, pg = dist_init()
+    L = lattice_of(args, "4,4,4,4")
+    g = O.Geom(L, (1, 1, 1, -1))
+    O.ranset(0, 1000003 * rank)
+    u = g.hot()
+    clov = g.clover_init(u, CSW * KAPPA)
+    g.flip_bc(u)
+    b = g.gauss_spinor(0, 0.5)
+    for _ in range(args.warmup):
+        g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, rest=0.0, maxiter=20, log=2)
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.cg("mtdagmt", np.zeros_like(b), b, u, clov, KAPPA, CSW * KAPPA, rest=0.0, maxiter=20, log=2)
+    mine = (time.perf_counter() - t0) / args.steps + 0.01 * rank    # a rank-dependent part, to see the max
+    step = allmax(pg, mine, local)
+    per_rank = [mine]
+    if pg is not None:
+        import torch
+        t = torch.zeros(world, dtype=torch.float64)
+        t[rank] = mine
+        pg.all_reduce(t)
+        per_rank = t.tolist()
+    if rank == 0:
+        print(json.dumps({"metric": "replica plumbing (CPU stand-in)", "value": step, "unit": "s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "per_rank_s": per_rank,
+                          "scaling": "weak", "config": {"workload": "plumbing", "lattice": list(L),
+                                                        "parallelism": "replicas x%d" % world}}))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def self_launch(args):
+    """bench.py --gpus N (N > 1) started without torchrun: start N ranks,
+    one per GPU, through torch.distributed.run on 127.0.0.1 with the same
+    arguments, and return their exit status.  Rank 0 prints the line."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -854,10 +934,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="solve",
-                    choices=["solve", "hmc", "batch", "shifts", "confio", "smp", "mpp"],
+                    choices=["solve", "hmc", "batch", "shifts", "confio", "smp", "mpp", "plumbing"],
                     help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories; "
                          "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128; "
-                         "confio: configuration files; smp, mpp: the reference's benchmark jobs")
+                         "confio: configuration files; smp, mpp: the reference's benchmark jobs; "
+                         "plumbing: CPU stand-in for testing the multi-process launch")
     ap.add_argument("--therm", type=int, default=10,
                     help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
     ap.add_argument("--ref-rhs", type=int, default=8, help="shifts: systems checked against an FP64 solve")
@@ -867,14 +948,20 @@ def main():
     ap.add_argument("--cool", type=int, default=-1,
                     help="conf_relax sweeps; -1: until the plaquette reaches %.2f" % PLAQ_TARGET)
     ap.add_argument("--tol", type=float, default=1e-10)
-    ap.add_argument("--fp64-steps", type=int, default=1)
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="timed e2e calls; 0: as many as --steps")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU seconds of the cpu_baseline's CG sample")
     ap.add_argument("--ref-maxiter", type=int, default=20000)
-    ap.add_argument("--ref-budget", type=float, default=90.0, help="seconds for the reference arm's CPU solve")
+    ap.add_argument("--ref-sample-seconds", type=float, default=1.5,
+                    help="reference arm: CPU seconds of each timed step's bounded CG sample (at least 10 iterations)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(self_launch(args))
+    if args.workload == "plumbing":
+        run_plumbing(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "hmc":
         run_hmc(args)

@@ -118,8 +118,12 @@ inline FastDiv make_fastdiv(unsigned d) {
   const unsigned long long m = ((1ull << 32) * ((1ull << l) - d)) / d + 1;
   return FastDiv{d, (unsigned)m, l};
 }
-__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
+__host__ __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
+#ifdef __CUDA_ARCH__
   return (__umulhi(n, f.m) + n) >> f.l;
+#else
+  return ((unsigned)(((unsigned long long)n * f.m) >> 32) + n) >> f.l;
+#endif
 }
 
 struct Geom {
@@ -143,7 +147,7 @@ struct Site {
   int base;  // i - x/2 : index offset of the (y,z,t) row
 };
 
-__device__ __forceinline__ Site site_coords(const Geom& g, int i, int parity) {
+__host__ __device__ __forceinline__ Site site_coords(const Geom& g, int i, int parity) {
   Site s;
   const int r = (int)fdiv((unsigned)i, g.dxh);
   const int xh = i - r * g.Lxh;
@@ -157,7 +161,7 @@ __device__ __forceinline__ Site site_coords(const Geom& g, int i, int parity) {
 }
 
 // index of the neighbour of site s in direction mu (fwd: +1, bwd: -1)
-__device__ __forceinline__ int neighbour(const Geom& g, const Site& s, int i, int mu, bool fwd) {
+__host__ __device__ __forceinline__ int neighbour(const Geom& g, const Site& s, int i, int mu, bool fwd) {
   if (mu == 0) {
     int x = s.x[0] + (fwd ? 1 : -1);
     if (x < 0) x += g.L[0];
@@ -173,7 +177,7 @@ __device__ __forceinline__ int neighbour(const Geom& g, const Site& s, int i, in
 
 // boundary sign of the link used by a hop: the forward hop uses U_mu(x), the
 // backward hop U_mu(x-mu); flip_bc negates links on the slice x_mu = L_mu-1.
-__device__ __forceinline__ int hop_sign(const Geom& g, const Site& s, int mu, bool fwd) {
+__host__ __device__ __forceinline__ int hop_sign(const Geom& g, const Site& s, int mu, bool fwd) {
   if (g.bcsign[mu] > 0) return 1;
   return (fwd ? s.x[mu] == g.L[mu] - 1 : s.x[mu] == 0) ? g.bcsign[mu] : 1;
 }

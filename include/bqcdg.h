@@ -346,12 +346,18 @@ int bqcdg_field_cdot_pairs(bqcdg_ctx *ctx, int n, const int *ha, const int *hb, 
  * cudaStream_t (NULL: the default stream); the call only enqueues work.
  *
  * Its two intermediate fields live in one static device array sized for
- * volh <= BQCDG_NOALLOC_MAX_VOLH (6.3 MB, held by every GPU that loads the
- * library until the process exits); larger lattices are rejected with
- * BQCDG_EINVAL.  The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current; make that first
- * call before any stream capture, and from one host thread at a time (the
- * look-up is not locked).  All calls on a device share the array and
+ * volh <= BQCDG_NOALLOC_MAX_VOLH (6.3 MB per device, held until the process
+ * exits); larger lattices are rejected with BQCDG_EINVAL.  The first call on
+ * a device looks up that array's device address (cudaGetSymbolAddress) with
+ * the device current.  Under CUDA's lazy module loading that look-up is also
+ * what loads the library's kernels on the device and allocates the array, so
+ * the first call is the one that may allocate and synchronise: make it before
+ * any stream capture, before a latency-critical region and before a pool or
+ * arena takes over the device's memory, and from one host thread at a time
+ * (the look-up is not locked).  The address is kept per device ordinal for
+ * the rest of the process: after a cudaDeviceReset, or under another CUDA
+ * context than the one current at the first call, it is stale and the entry
+ * point must not be called again.  All calls on a device share the array and
  * it keeps the last call's contents: calls that overlap on the GPU race.
  * Nothing in it needs to start at zero, since each call writes every site it
  * later reads. */

@@ -136,4 +136,8 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: first argument, else $BQCD_REFERENCE
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BQCD_REFERENCE")
+    if not src:
+        sys.exit("usage: make_golden.py <reference checkout>  (or set BQCD_REFERENCE)")
+    main(src)

@@ -77,3 +77,24 @@ def test_python_mirror_fails_loudly_without_gpu(bq):
         pytest.skip("a GPU is present")
     with pytest.raises(bq.BqcdgError):
         bq.Lattice((4, 4, 4, 4))
+
+
+def test_noalloc_argument_and_size_checks(so, bq):
+    """bqcdg_mdagm_noalloc rejects missing arguments and a lattice larger
+    than its static scratch before it touches a device."""
+    lib = C.CDLL(so)
+    f = lib.bqcdg_mdagm_noalloc
+    f.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                  C.POINTER(bq.Params), C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    bc = (C.c_int * 4)(1, 1, 1, -1)
+    one = C.c_void_p(1)            # never dereferenced: the checks come first
+    big = (C.c_int * 4)(16, 16, 16, 16)     # volh 32768 > BQCDG_NOALLOC_MAX_VOLH
+    prm = bq.Params(0.13, 0.0, 0.0, 0.0)
+    assert f(big, bc, one, one, one, C.byref(prm), one, one, None) == bq.EINVAL
+    small = (C.c_int * 4)(4, 4, 4, 4)
+    assert f(small, bc, None, one, one, C.byref(prm), one, one, None) == bq.EINVAL
+    assert f(small, bc, one, one, one, None, one, one, None) == bq.EINVAL
+    assert f((C.c_int * 4)(5, 4, 4, 4), bc, one, one, one, C.byref(prm), one, one, None) == bq.EINVAL
+    clov = bq.Params(0.13, 0.25, 0.0, 0.0)  # csw != 0 needs both clover parts
+    assert f(small, bc, one, None, one, C.byref(clov), one, one, None) == bq.ENOCLOVER

@@ -97,6 +97,19 @@ def test_clover_operators(setup, bq, name):
 
 
 @pytest.mark.parametrize("name", OPS)
+def test_clover_operators_with_h(setup, bq, name):
+    """Clover and h together (m_tilde.F90:55-58, 92-95): h_mult_b after
+    A_oo^-1 in the first half, b = -kappa^2/(1+h^2) in the second."""
+    g, lat = setup["g"], setup["lat"]
+    h, rho = 0.05, 0.1
+    para = bq.HmcPara(kappa=setup["kappa"], csw=setup["csw"], h=h, rho=rho)
+    psi = g.gauss_spinor(0)
+    ref = g.op(name, psi, setup["uf"], setup["clov"], setup["kappa"], para.csw_kappa, h, rho)
+    got = getattr(lat, name)(psi, para)
+    assert rel(got, ref) < TOL64
+
+
+@pytest.mark.parametrize("name", OPS)
 def test_wilson_operators_with_h(setup, bq, name):
     """csw = 0 selects the Wilson operator, where h_mult adds i h gamma_5."""
     g, lat = setup["g"], setup["lat"]

@@ -56,8 +56,8 @@ def test_barrier_and_max_over_two_ranks():
 def test_reference_arm_under_torchrun_prints_one_line():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(free_port()), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--lattice", "4,4,4,8", "--steps", "1", "--warmup", "3", "--cpu-seconds", "0.2",
-           "--ref-budget", "5"]
+           "--gpus", "2", "--lattice", "4,4,4,8", "--steps", "1", "--warmup", "3", "--ref-sample-seconds",
+           "0.2"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -66,3 +66,21 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["value"] > 0 and d["e2e"]["value"] == d["value"]
     assert d["cpu_baseline"]["kind"] == "port"
+    fs = d["full_solve"]
+    assert fs["converged"] and fs["true_rel_residual"] < 1e-9 and fs["iterations"] > 10
+    for k in ("lattice", "volh", "sweeps", "plaquette", "parallelism"):
+        assert k in d["config"]
+
+
+def test_bench_launches_its_own_ranks():
+    """bench.py --gpus 2 without torchrun starts two ranks itself; the line
+    comes from rank 0 alone, with n_gpus 2 and the max over the ranks."""
+    cmd = [sys.executable, "bench.py", "--gpus", "2", "--workload", "plumbing", "--steps", "2", "--warmup", "1"]
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and len(d["per_rank_s"]) == 2
+    assert d["value"] == max(d["per_rank_s"]) and d["per_rank_s"][1] > 0.01

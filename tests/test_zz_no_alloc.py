@@ -5,8 +5,9 @@ It serves callers that cannot let the library allocate: everything it needs
 besides the caller's inputs and outputs sits in a fixed static device array.
 Its result must equal the context-based entry points (bqcdg_mtdagmt /
 bqcdg_w_dagger_w on host arrays) to the FP64 operator tolerance, on two calls
-in a row (the second reuses the static scratch left by the first), and a
-lattice larger than the stated maximum must be rejected.
+in a row (the second reuses the static scratch left by the first), and the
+second call must leave the device's free memory unchanged.  (Its argument
+and size checks need no device and run in tests/test_abi.py.)
 """
 import ctypes as C
 
@@ -83,18 +84,17 @@ def test_noalloc_matches_context_entry_point_twice(oracle, bq, fn, rho):
         for call in range(2):
             psi = g.gauss_spinor(0)
             d_in.copy_(dev(spinor_layout(psi, volh), torch))
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             st = fn(Li, bci, d_u.data_ptr(), d_a.data_ptr(), d_ai.data_ptr(), C.byref(prm), d_in.data_ptr(),
                     d_out.data_ptr(), None)
             assert st == bq.OK
             torch.cuda.synchronize()
+            if call == 1:
+                # after the first call (which loads the kernels and the static
+                # array) a call takes no device memory
+                assert torch.cuda.mem_get_info()[0] == free_before
             got = spinor_from_layout(d_out.cpu().numpy(), volh)
             ref = lat.w_dagger_w(psi, para) if rho else lat.mtdagmt(psi, para)
             assert np.linalg.norm(got - ref) <= TOL64 * np.linalg.norm(ref), call
 
-
-def test_noalloc_rejects_lattices_beyond_the_static_scratch(bq, fn):
-    L = (16, 16, 16, 16)           # volh 32768 > BQCDG_NOALLOC_MAX_VOLH
-    prm = bq.Params(0.13, 0.0, 0.0, 0.0)
-    one = C.c_void_p(1)            # never dereferenced: the size check comes first
-    st = fn((C.c_int * 4)(*L), (C.c_int * 4)(1, 1, 1, -1), one, one, one, C.byref(prm), one, one, None)
-    assert st == bq.EINVAL
