@@ -21,6 +21,7 @@ the data path; the step time is the max over ranks.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -475,12 +476,23 @@ def run_hmc(args):
     b2 = lat.field_cdot(hb, hb).real   # |phi|^2 scale of a unit-variance field
     hmc = Hmc(lat, beta=beta, kappa=kappa, csw=CSW, rho=kappa / kshift - 1, traj_length=1.0, ntau=20, m_scale=5,
               model="C", rest=1e-20 * b2, maxiter=100000, solver="mixed")
+    # dynamical thermalisation: forced-accept N_f = 2 trajectories of the
+    # same algorithm, which bring the configuration to the fermionic
+    # equilibrium, where dH is O(1)
+    therm_dyn = []
+    for k in range(args.therm_dyn):
+        rec = hmc.trajectory(force_accept=True)
+        therm_dyn.append({"dh": round(rec["dh"], 3), "plaq": round(1.0 - rec["plaq_energy"], 5)})
+        print("hmc: thermalisation %d dH %.3f plaquette %.5f" % (k, rec["dh"], 1.0 - rec["plaq_energy"]),
+              file=sys.stderr, flush=True)
     recs = []
     for k in range(args.warmup + args.steps):
         barrier(pg, local)
         t0 = time.perf_counter()
         rec = hmc.trajectory()
         rec["seconds"] = allmax(pg, time.perf_counter() - t0, local)
+        print("hmc: trajectory %d dH %.4f accepted %d %.2f s" % (k, rec["dh"], rec["accepted"], rec["seconds"]),
+              file=sys.stderr, flush=True)
         if k >= args.warmup:
             recs.append(rec)
     if rank == 0:
@@ -491,14 +503,19 @@ def run_hmc(args):
                "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / len(secs), 1),
                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64 (int16/f32 sloppy solves)", "data": "synthetic: hot start + %d conf_relax sweep(s), "
-               "then %d forced-accept pure-gauge trajectories (plaquettes %s)" % (lat.sweeps, args.therm, therm),
+               "then %d forced-accept pure-gauge trajectories (plaquettes %s), then %d forced-accept N_f=2 "
+               "trajectories of the measured algorithm" % (lat.sweeps, args.therm, therm, args.therm_dyn),
                "config": {"workload": "HMC model C, lattice %s, kappa %.4f, kappa_shift %.2f (rho %.5f), c_sw %.4f, "
                                       "beta %.2f, tau 1, 20x5 steps" % ("x".join(map(str, L)), kappa, kshift,
                                                                       kappa / kshift - 1, CSW, beta),
                           "parallelism": "replicas x%d" % world},
                "trajectories": [{k: r[k] for k in ("accepted", "dh", "plaq_energy", "it_f1", "it_f2", "cg_calls",
                                                    "cg_it_max", "seconds")} for r in recs],
-               "acceptance": sum(1 for r in recs if r["accepted"]) / len(recs)}
+               "acceptance": sum(1 for r in recs if r["accepted"]) / len(recs),
+               "dh_mean": sum(r["dh"] for r in recs) / len(recs),
+               "dh_abs_max": max(abs(r["dh"]) for r in recs),
+               "exp_minus_dh_mean": sum(math.exp(-r["dh"]) for r in recs) / len(recs),
+               "thermalisation_dynamical": therm_dyn}
         print(json.dumps(out))
     lat.close()
     if pg is not None:
@@ -941,6 +958,8 @@ def main():
                          "plumbing: CPU stand-in for testing the multi-process launch")
     ap.add_argument("--therm", type=int, default=10,
                     help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
+    ap.add_argument("--therm-dyn", type=int, default=30,
+                    help="hmc: forced-accept N_f=2 trajectories after the pure-gauge ones, before the measured ones")
     ap.add_argument("--ref-rhs", type=int, default=8, help="shifts: systems checked against an FP64 solve")
     ap.add_argument("--lattice", default=None,
                     help="x,y,z,t; default 32,32,32,64 (solve), 24,24,24,48 (hmc), 48,48,48,96 (batch), "

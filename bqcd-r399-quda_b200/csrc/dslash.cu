@@ -23,10 +23,17 @@ namespace bqcdg {
 #ifndef BQCDG_SLOPPY_MIN_BLOCKS2
 #define BQCDG_SLOPPY_MIN_BLOCKS2 5
 #endif
+// The int16 passes load all eight links of their site up front
+// (wilson_hop_lf), which takes about 120 registers: 4 CTAs per SM.
+#ifndef BQCDG_HALF_MIN_BLOCKS
+#define BQCDG_HALF_MIN_BLOCKS 4
+#endif
 template <Prec P>
 struct Occ {
-  static constexpr int min_blocks = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS;
-  static constexpr int min_blocks2 = P == Prec::F64 ? 1 : BQCDG_SLOPPY_MIN_BLOCKS2;
+  static constexpr int min_blocks =
+      P == Prec::F64 ? 1 : (P == Prec::F16 ? BQCDG_HALF_MIN_BLOCKS : BQCDG_SLOPPY_MIN_BLOCKS);
+  static constexpr int min_blocks2 =
+      P == Prec::F64 ? 1 : (P == Prec::F16 ? BQCDG_HALF_MIN_BLOCKS : BQCDG_SLOPPY_MIN_BLOCKS2);
 };
 
 // ---------------------------------------------------------------------------
@@ -167,7 +174,8 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
   Site st = site_coords(g, i, 1);
   Spinor<R> b;
   zero(b);
-  wilson_hop<P, DAG>(g, 1, i, st, in, U, b);
+  if constexpr (P == Prec::F16) wilson_hop_lf<DAG>(g, 1, i, st, in, U, b);
+  else wilson_hop<P, DAG>(g, 1, i, st, in, U, b);
   R osc = 1;  // a common factor of the output, folded into its storage scale
   if (has_clover) {
     Spinor<R> y;
@@ -231,7 +239,8 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
     }
   }
   const Site st = site_coords(g, i, 0);
-  wilson_hop<P, DAG>(g, 0, i, st, t, U, out, (R)bcoef);
+  if constexpr (P == Prec::F16) wilson_hop_lf<DAG>(g, 0, i, st, t, U, out, (R)bcoef);
+  else wilson_hop<P, DAG>(g, 0, i, st, t, U, out, (R)bcoef);
 }
 
 template <Prec P, bool DAG, bool REDUCE>
