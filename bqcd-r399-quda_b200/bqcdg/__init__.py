@@ -155,6 +155,15 @@ def _lib_handle():
         L.bqcdg_field_cdot.argtypes = [vp, i, i, pd, pd]
         L.bqcdg_field_caxpby.argtypes = [vp, i, d, d, d, i]
         L.bqcdg_field_cdot_pairs.argtypes = [vp, i, P(C.c_int), P(C.c_int), pd, pd]
+        L.bqcdg_dd_create_local.argtypes = [P(vp), P(C.c_int), P(C.c_int), i, i]
+        L.bqcdg_dd_nccl_unique_id.argtypes = [C.c_char_p]
+        L.bqcdg_dd_create_nccl.argtypes = [P(vp), P(C.c_int), P(C.c_int), i, i, i, C.c_char_p]
+        L.bqcdg_dd_destroy.argtypes = [vp]
+        L.bqcdg_dd_volh.argtypes = [vp]
+        L.bqcdg_dd_load_gauge.argtypes = [vp, dp, i]
+        L.bqcdg_dd_load_clover.argtypes = [vp, dp, dp]
+        L.bqcdg_dd_op.argtypes = [vp, i, dp, dp, P(Params)]
+        L.bqcdg_dd_cg.argtypes = [vp, dp, dp, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
         _LIB = L
     return _LIB
 
@@ -614,3 +623,77 @@ class Lattice:
         _check(lib().bqcdg_time_pass_batch(self.h, k, (C.c_int * k)(*hins), C.byref(prm), precision,
                                            rhs_per_thread, n, C.byref(ms)), "time_pass_batch")
         return ms.value
+
+
+class SlabDecomposition:
+    """The lattice cut along t into nranks slabs (bqcdg_dd_* of bqcdg.h), FP64.
+
+    SlabDecomposition.local(L, nranks): every slab in this process on one
+    device (host arrays are the global ones).  SlabDecomposition.nccl(L,
+    nranks, rank, uid): this process's slab, the others in their own
+    processes over NCCL (host arrays are the slab's; uid from
+    nccl_unique_id() on rank 0, passed to the others by the caller)."""
+
+    OPS = {"mtil": 0, "mtil_dag": 1, "mtdagmt": 2, "w_mult": 3, "w_mult_dag": 4, "w_dagger_w": 5, "d": 6,
+           "d_dag": 7}
+
+    def __init__(self, handle, L, nranks):
+        self.h = handle
+        self.L = tuple(L)
+        self.nranks = nranks
+        self.volh = lib().bqcdg_dd_volh(self.h)
+
+    @classmethod
+    def local(cls, L, nranks, bc=(1, 1, 1, -1), device=0):
+        h = C.c_void_p()
+        _check(lib().bqcdg_dd_create_local(C.byref(h), (C.c_int * 4)(*L), (C.c_int * 4)(*bc), nranks, device),
+               "dd_create_local")
+        return cls(h, L, nranks)
+
+    @staticmethod
+    def nccl_unique_id():
+        buf = C.create_string_buffer(128)
+        _check(lib().bqcdg_dd_nccl_unique_id(buf), "dd_nccl_unique_id")
+        return buf.raw
+
+    @classmethod
+    def nccl(cls, L, nranks, rank, uid, bc=(1, 1, 1, -1), device=0):
+        h = C.c_void_p()
+        _check(lib().bqcdg_dd_create_nccl(C.byref(h), (C.c_int * 4)(*L), (C.c_int * 4)(*bc), nranks, rank, device,
+                                          uid), "dd_create_nccl")
+        return cls(h, L, nranks)
+
+    def close(self):
+        if self.h:
+            lib().bqcdg_dd_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def load_gauge(self, u, flipped):
+        _check(lib().bqcdg_dd_load_gauge(self.h, _ptr(u, np.complex128), int(flipped)), "dd_load_gauge")
+
+    def load_clover(self, a, ainv):
+        _check(lib().bqcdg_dd_load_clover(self.h, _ptr(a, np.complex128), _ptr(ainv, np.complex128)),
+               "dd_load_clover")
+
+    def op(self, name, inp, para):
+        out = np.zeros((self.volh, 3, 4), np.complex128)
+        prm = para.params() if isinstance(para, HmcPara) else para
+        _check(lib().bqcdg_dd_op(self.h, self.OPS[name], out.ctypes.data, _ptr(inp, np.complex128), C.byref(prm)),
+               "dd_op")
+        return out
+
+    def cg(self, x, b, para, rest, maxiter=1000, log=0, rho=None):
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        it = C.c_int()
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        cp = CgPara(rest, maxiter, log)
+        _check(lib().bqcdg_dd_cg(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(cp),
+                                 C.byref(it), C.byref(info)), "dd_cg")
+        return x, it.value, info

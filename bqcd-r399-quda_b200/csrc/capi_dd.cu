@@ -1,0 +1,487 @@
+// capi_dd.cu -- the time-slab domain decomposition behind the bqcdg_dd_* entry
+// points of include/bqcdg.h: one context per slab (a lattice of Lt / nranks
+// time slices), the face exchange before every stencil pass, the global sums
+// of the CG, and two ways for the slabs to talk:
+//
+//   local  all slabs of the lattice in this process on one device; a face is
+//          packed straight into the neighbour slab's ghost buffer and a global
+//          sum adds the slabs' partial sums on the host in rank order.  This
+//          is how the decomposition runs (and is tested) on one GPU.
+//   nccl   one slab per process and GPU; faces go by ncclSend / ncclRecv into
+//          the ghost buffers and global sums by ncclAllReduce, all on the
+//          slab's stream.  libnccl.so.2 is opened at run time (the one a
+//          process such as PyTorch has loaded already, if any).
+//
+// The reference does the same over MPI: project to half spinors
+// (d/D21.F90:53), exchange the faces (xbound, comm/xbound_mpi.F90:418-461),
+// compute (d/D21.F90:58-72), and global_sum the CG scalars (cg.F90:91,97,109).
+#include <dlfcn.h>
+#include <nccl.h>
+
+#include "ctx.cuh"
+#include "decomp.cuh"
+
+namespace bqcdg {
+void launch_dd_pack(const Geom& g, const DdGeom& d, bool dag, const double2* in, double2* to_prev, double2* to_next,
+                    cudaStream_t s);
+void launch_dd_pack_links(const Geom& g, const DdGeom& d, const double2* gauge, double2* to_next, cudaStream_t s);
+void launch_dd_dslash(const Geom& g, const DdGeom& d, int e, bool dag, double2* out, const double2* in,
+                      const double2* gauge, cudaStream_t s);
+void launch_dd_pass1(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* in, const double2* gauge,
+                     const double2* ainv, const OpParams& op, cudaStream_t s);
+void launch_dd_pass2(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* t, const double2* in,
+                     const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s);
+}  // namespace bqcdg
+
+using namespace bqcdg_host;
+
+namespace {
+
+// the NCCL calls this file makes, resolved from libnccl.so.2 at run time
+struct NcclApi {
+  void* lib = nullptr;
+  ncclResult_t (*getUniqueId)(ncclUniqueId*) = nullptr;
+  ncclResult_t (*commInitRank)(ncclComm_t*, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*commDestroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*groupStart)() = nullptr;
+  ncclResult_t (*groupEnd)() = nullptr;
+  ncclResult_t (*send)(const void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*recv)(void*, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*allReduce)(const void*, void*, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                            cudaStream_t) = nullptr;
+  bool load() {
+    if (lib) return true;
+    lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!lib) return false;
+    getUniqueId = (decltype(getUniqueId))dlsym(lib, "ncclGetUniqueId");
+    commInitRank = (decltype(commInitRank))dlsym(lib, "ncclCommInitRank");
+    commDestroy = (decltype(commDestroy))dlsym(lib, "ncclCommDestroy");
+    groupStart = (decltype(groupStart))dlsym(lib, "ncclGroupStart");
+    groupEnd = (decltype(groupEnd))dlsym(lib, "ncclGroupEnd");
+    send = (decltype(send))dlsym(lib, "ncclSend");
+    recv = (decltype(recv))dlsym(lib, "ncclRecv");
+    allReduce = (decltype(allReduce))dlsym(lib, "ncclAllReduce");
+    return getUniqueId && commInitRank && commDestroy && groupStart && groupEnd && send && recv && allReduce;
+  }
+};
+NcclApi g_nccl;
+
+// device buffers of one slab for the exchange
+struct SlabBufs {
+  double2* ghost_fwd = nullptr;   // [6][V3h]
+  double2* ghost_bwd = nullptr;   // [6][V3h]
+  double2* ghost_link = nullptr;  // [2][9][V3h]
+  double2* send_prev = nullptr;   // nccl: [6][V3h] for rank-1
+  double2* send_next = nullptr;   // nccl: [6][V3h] for rank+1
+  double2* send_links = nullptr;  // nccl: [2][9][V3h] for rank+1
+};
+
+}  // namespace
+
+struct bqcdg_dd {
+  bool nccl = false;
+  int nranks = 1, rank0 = 0;  // rank of slabs[0]
+  int L[4] = {0, 0, 0, 0}, bc[4] = {0, 0, 0, 0};
+  int Lt_loc = 0, V3h = 0, volh_loc = 0;
+  std::vector<bqcdg_ctx*> slabs;
+  std::vector<SlabBufs> bufs;
+  cudaStream_t stream = nullptr;  // every slab works on the first slab's stream
+  ncclComm_t comm = nullptr;
+  double* dsum = nullptr;         // nccl: device scalars of the global sums
+  std::vector<double> hsum;
+
+  int nslabs() const { return (int)slabs.size(); }
+  DdGeom geom(int s) const {
+    DdGeom d{};
+    d.nranks = nranks;
+    d.rank = rank0 + s;
+    d.Lt_glob = L[3];
+    d.t0 = (rank0 + s) * Lt_loc;
+    d.V3h = V3h;
+    d.bct = bc[3];
+    d.ghost_fwd = bufs[s].ghost_fwd;
+    d.ghost_bwd = bufs[s].ghost_bwd;
+    d.ghost_link = bufs[s].ghost_link;
+    return d;
+  }
+};
+
+namespace {
+
+int dd_check(bqcdg_dd* dd) { return dd && !dd->slabs.empty() ? BQCDG_OK : BQCDG_EINVAL; }
+
+// the faces of field f[s] of every slab, for passes with (dag) or without
+// the dagger, into the ghost buffers of their neighbours
+int dd_exchange(bqcdg_dd* dd, const std::vector<double2*>& f, bool dag) {
+  const int n = dd->nslabs();
+  if (!dd->nccl) {
+    for (int s = 0; s < n; s++) {
+      const int prev = (s + n - 1) % n, next = (s + 1) % n;
+      launch_dd_pack(dd->slabs[s]->g, dd->geom(s), dag, f[s], dd->bufs[prev].ghost_fwd, dd->bufs[next].ghost_bwd,
+                     dd->stream);
+    }
+    CKL();
+    return BQCDG_OK;
+  }
+  SlabBufs& b = dd->bufs[0];
+  launch_dd_pack(dd->slabs[0]->g, dd->geom(0), dag, f[0], b.send_prev, b.send_next, dd->stream);
+  CKL();
+  const int r = dd->rank0, prev = (r + dd->nranks - 1) % dd->nranks, next = (r + 1) % dd->nranks;
+  const size_t cnt = (size_t)6 * dd->V3h * 2;  // doubles per face
+  if (g_nccl.groupStart() != ncclSuccess) return BQCDG_ECUDA;
+  ncclResult_t e = g_nccl.send(b.send_prev, cnt, ncclDouble, prev, dd->comm, dd->stream);
+  if (e == ncclSuccess) e = g_nccl.recv(b.ghost_fwd, cnt, ncclDouble, next, dd->comm, dd->stream);
+  if (e == ncclSuccess) e = g_nccl.send(b.send_next, cnt, ncclDouble, next, dd->comm, dd->stream);
+  if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclDouble, prev, dd->comm, dd->stream);
+  if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
+  return BQCDG_OK;
+}
+
+// U_t of each slab's last slice into the ghost links of the next slab
+int dd_exchange_links(bqcdg_dd* dd) {
+  const int n = dd->nslabs();
+  if (!dd->nccl) {
+    for (int s = 0; s < n; s++)
+      launch_dd_pack_links(dd->slabs[s]->g, dd->geom(s), dd->slabs[s]->gauge64, dd->bufs[(s + 1) % n].ghost_link,
+                           dd->stream);
+    CKL();
+    return BQCDG_OK;
+  }
+  SlabBufs& b = dd->bufs[0];
+  launch_dd_pack_links(dd->slabs[0]->g, dd->geom(0), dd->slabs[0]->gauge64, b.send_links, dd->stream);
+  CKL();
+  const int r = dd->rank0, prev = (r + dd->nranks - 1) % dd->nranks, next = (r + 1) % dd->nranks;
+  const size_t cnt = (size_t)18 * dd->V3h * 2;
+  if (g_nccl.groupStart() != ncclSuccess) return BQCDG_ECUDA;
+  ncclResult_t e = g_nccl.send(b.send_links, cnt, ncclDouble, next, dd->comm, dd->stream);
+  if (e == ncclSuccess) e = g_nccl.recv(b.ghost_link, cnt, ncclDouble, prev, dd->comm, dd->stream);
+  if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
+  return BQCDG_OK;
+}
+
+// global sums of k local values per slab (dres[0..k-1] of each slab, written
+// on dd->stream); out[0..k-1] on the host.  local: the slabs' values added in
+// rank order; nccl: ncclAllReduce.
+int dd_global_sum(bqcdg_dd* dd, int k, double* out) {
+  if (!dd->nccl) {
+    for (int j = 0; j < k; j++) out[j] = 0.0;
+    CK(cudaStreamSynchronize(dd->stream));
+    for (int s = 0; s < dd->nslabs(); s++) {
+      double v[4];
+      CK(cudaMemcpy(v, dd->slabs[s]->dres, k * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int j = 0; j < k; j++) out[j] += v[j];
+    }
+    return BQCDG_OK;
+  }
+  if (g_nccl.allReduce(dd->slabs[0]->dres, dd->dsum, k, ncclDouble, ncclSum, dd->comm, dd->stream) != ncclSuccess)
+    return BQCDG_ECUDA;
+  CK(cudaMemcpyAsync(out, dd->dsum, k * sizeof(double), cudaMemcpyDeviceToHost, dd->stream));
+  CK(cudaStreamSynchronize(dd->stream));
+  return BQCDG_OK;
+}
+
+double2* aee_of_slab(bqcdg_ctx* c) { return c->A[0]; }
+double2* ainv_oo_of_slab(bqcdg_ctx* c) { return c->Ainv[1]; }
+
+// out = mtil / mtil_dag in on every slab (t: odd work field of each slab)
+int dd_mtil(bqcdg_dd* dd, bool dag, const std::vector<double2*>& out, const std::vector<double2*>& in,
+            const std::vector<double2*>& t, const OpParams& op) {
+  int st;
+  if ((st = dd_exchange(dd, in, dag))) return st;
+  for (int s = 0; s < dd->nslabs(); s++) {
+    bqcdg_ctx* c = dd->slabs[s];
+    launch_dd_pass1(c->g, dd->geom(s), dag, t[s], in[s], c->gauge64, ainv_oo_of_slab(c), op, dd->stream);
+  }
+  CKL();
+  if ((st = dd_exchange(dd, t, dag))) return st;
+  for (int s = 0; s < dd->nslabs(); s++) {
+    bqcdg_ctx* c = dd->slabs[s];
+    launch_dd_pass2(c->g, dd->geom(s), dag, out[s], t[s], in[s], c->gauge64, aee_of_slab(c), op, dd->stream);
+  }
+  CKL();
+  return BQCDG_OK;
+}
+
+int dd_mdagm(bqcdg_dd* dd, const std::vector<double2*>& out, const std::vector<double2*>& in,
+             const std::vector<double2*>& t, const std::vector<double2*>& q, const OpParams& op) {
+  int st = dd_mtil(dd, false, q, in, t, op);
+  return st ? st : dd_mtil(dd, true, out, q, t, op);
+}
+
+// work field k of every slab
+int dd_fields(bqcdg_dd* dd, int k, std::vector<double2*>& v) {
+  v.resize(dd->nslabs());
+  for (int s = 0; s < dd->nslabs(); s++)
+    if (!(v[s] = dd->slabs[s]->sp64(k))) return BQCDG_ENOMEM;
+  return BQCDG_OK;
+}
+
+// host spinors: local groups take the global array (slab s = rows
+// [s volh_loc, (s+1) volh_loc)), nccl the slab's own
+int dd_upload(bqcdg_dd* dd, const double* host, const std::vector<double2*>& dev) {
+  for (int s = 0; s < dd->nslabs(); s++) {
+    int st = upload_spinor(dd->slabs[s], host + (size_t)s * dd->volh_loc * 24, dev[s]);
+    if (st) return st;
+  }
+  for (bqcdg_ctx* c : dd->slabs) CK(cudaStreamSynchronize(c->stream));
+  return BQCDG_OK;
+}
+int dd_download(bqcdg_dd* dd, const std::vector<double2*>& dev, double* host) {
+  CK(cudaStreamSynchronize(dd->stream));
+  for (int s = 0; s < dd->nslabs(); s++) {
+    int st = download_spinor(dd->slabs[s], dev[s], host + (size_t)s * dd->volh_loc * 24);
+    if (st) return st;
+  }
+  return BQCDG_OK;
+}
+
+int dd_create(bqcdg_dd** out, const int L[4], const int bc[4], int nranks, int rank, int nslabs, int device) {
+  if (!out || !L || !bc || nranks < 1) return BQCDG_EINVAL;
+  *out = nullptr;
+  for (int d = 0; d < 4; d++)
+    if (L[d] <= 0 || L[d] % 2 || (bc[d] != 1 && bc[d] != -1)) return BQCDG_EINVAL;
+  if (L[3] % nranks || (L[3] / nranks) % 2) return BQCDG_EINVAL;  // even slabs keep the parity
+  if (rank < 0 || rank + nslabs > nranks) return BQCDG_EINVAL;
+  bqcdg_dd* dd = new bqcdg_dd();
+  dd->nranks = nranks;
+  dd->rank0 = rank;
+  for (int d = 0; d < 4; d++) {
+    dd->L[d] = L[d];
+    dd->bc[d] = bc[d];
+  }
+  dd->Lt_loc = L[3] / nranks;
+  dd->V3h = L[0] * L[1] * L[2] / 2;
+  dd->volh_loc = dd->V3h * dd->Lt_loc;
+  const int Lloc[4] = {L[0], L[1], L[2], dd->Lt_loc};
+  for (int s = 0; s < nslabs; s++) {
+    bqcdg_ctx* c = nullptr;
+    int st = bqcdg_create(&c, Lloc, bc, device);
+    if (st) {
+      bqcdg_dd_destroy(dd);
+      return st;
+    }
+    dd->slabs.push_back(c);
+    dd->bufs.push_back(SlabBufs{});
+  }
+  dd->stream = dd->slabs[0]->stream;
+  const size_t face = (size_t)6 * dd->V3h * sizeof(double2), links = (size_t)18 * dd->V3h * sizeof(double2);
+  for (int s = 0; s < nslabs; s++) {
+    bqcdg_ctx* c = dd->slabs[s];
+    SlabBufs& b = dd->bufs[s];
+    cudaError_t e = c->alloc((void**)&b.ghost_fwd, face);
+    if (e == cudaSuccess) e = c->alloc((void**)&b.ghost_bwd, face);
+    if (e == cudaSuccess) e = c->alloc((void**)&b.ghost_link, links);
+    if (e != cudaSuccess) {
+      bqcdg_dd_destroy(dd);
+      return status_from_cuda(e);
+    }
+  }
+  *out = dd;
+  return BQCDG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bqcdg_dd_create_local(bqcdg_dd** dd, const int L[4], const int bc[4], int nranks, int device) {
+  return dd_create(dd, L, bc, nranks, 0, nranks, device);
+}
+
+int bqcdg_dd_nccl_unique_id(char* id) {
+  if (!id) return BQCDG_EINVAL;
+  if (!g_nccl.load()) return BQCDG_EUNSUPPORTED;
+  ncclUniqueId u;
+  if (g_nccl.getUniqueId(&u) != ncclSuccess) return BQCDG_ECUDA;
+  std::memcpy(id, u.internal, sizeof(u.internal));
+  return BQCDG_OK;
+}
+
+int bqcdg_dd_create_nccl(bqcdg_dd** out, const int L[4], const int bc[4], int nranks, int rank, int device,
+                         const char* id) {
+  if (!id) return BQCDG_EINVAL;
+  if (!g_nccl.load()) return BQCDG_EUNSUPPORTED;
+  int st = dd_create(out, L, bc, nranks, rank, 1, device);
+  if (st) return st;
+  bqcdg_dd* dd = *out;
+  dd->nccl = true;
+  bqcdg_ctx* c = dd->slabs[0];
+  SlabBufs& b = dd->bufs[0];
+  const size_t face = (size_t)6 * dd->V3h * sizeof(double2), links = (size_t)18 * dd->V3h * sizeof(double2);
+  cudaError_t e = c->alloc((void**)&b.send_prev, face);
+  if (e == cudaSuccess) e = c->alloc((void**)&b.send_next, face);
+  if (e == cudaSuccess) e = c->alloc((void**)&b.send_links, links);
+  if (e == cudaSuccess) e = c->alloc((void**)&dd->dsum, 4 * sizeof(double));
+  ncclUniqueId u;
+  std::memcpy(u.internal, id, sizeof(u.internal));
+  if (e == cudaSuccess && g_nccl.commInitRank(&dd->comm, nranks, u, rank) != ncclSuccess) e = cudaErrorUnknown;
+  if (e != cudaSuccess) {
+    bqcdg_dd_destroy(dd);
+    *out = nullptr;
+    return BQCDG_ECUDA;
+  }
+  return BQCDG_OK;
+}
+
+int bqcdg_dd_destroy(bqcdg_dd* dd) {
+  if (!dd) return BQCDG_EINVAL;
+  if (dd->comm) g_nccl.commDestroy(dd->comm);
+  for (bqcdg_ctx* c : dd->slabs) bqcdg_destroy(c);  // frees every buffer the slab allocated
+  delete dd;
+  return BQCDG_OK;
+}
+
+int bqcdg_dd_volh(const bqcdg_dd* dd) { return dd ? dd->volh_loc * (int)dd->slabs.size() : -1; }
+
+int bqcdg_dd_load_gauge(bqcdg_dd* dd, const double* u, int flipped) {
+  int st = dd_check(dd);
+  if (st || !u) return BQCDG_EINVAL;
+  const size_t nloc = (size_t)dd->volh_loc * 18;  // doubles of one (mu, parity) block of a slab
+  const size_t nhost = nloc * dd->nslabs();
+  std::vector<double> tmp(8 * nloc);
+  for (int s = 0; s < dd->nslabs(); s++) {
+    for (int me = 0; me < 8; me++) std::memcpy(tmp.data() + me * nloc, u + me * nhost + s * nloc, nloc * 8);
+    // only the last slab holds the global last time slice, where flip_bc put its sign
+    const bool last = dd->rank0 + s == dd->nranks - 1;
+    if ((st = bqcdg_load_gauge(dd->slabs[s], tmp.data(), flipped && last ? 1 : 0))) return st;
+  }
+  if ((st = dd_exchange_links(dd))) return st;
+  CK(cudaStreamSynchronize(dd->stream));
+  return BQCDG_OK;
+}
+
+int bqcdg_dd_load_clover(bqcdg_dd* dd, const double* a, const double* ainv) {
+  int st = dd_check(dd);
+  if (st || !a || !ainv) return BQCDG_EINVAL;
+  const size_t nloc = (size_t)dd->volh_loc * 72;  // doubles of one parity of a slab
+  const size_t nhost = nloc * dd->nslabs();
+  std::vector<double> ta(2 * nloc), ti(2 * nloc);
+  for (int s = 0; s < dd->nslabs(); s++) {
+    for (int eo = 0; eo < 2; eo++) {
+      std::memcpy(ta.data() + eo * nloc, a + eo * nhost + s * nloc, nloc * 8);
+      std::memcpy(ti.data() + eo * nloc, ainv + eo * nhost + s * nloc, nloc * 8);
+    }
+    if ((st = bqcdg_load_clover(dd->slabs[s], ta.data(), ti.data(), nullptr))) return st;
+    CK(cudaStreamSynchronize(dd->slabs[s]->stream));
+  }
+  return BQCDG_OK;
+}
+
+int bqcdg_dd_op(bqcdg_dd* dd, int which, double* out, const double* in, const bqcdg_params* p) {
+  int st = dd_check(dd);
+  if (st || !out || !in || !p || which < 0 || which > 7) return BQCDG_EINVAL;
+  for (bqcdg_ctx* c : dd->slabs) {
+    if (!c->have_gauge) return BQCDG_ENOGAUGE;
+    if (p->csw_kappa != 0.0 && which < 6 && (!c->have_A[0] || !c->have_Ainv[1])) return BQCDG_ENOCLOVER;
+  }
+  CK(cudaSetDevice(dd->slabs[0]->device));
+  std::vector<double2*> vin, vout, t, q;
+  if ((st = dd_fields(dd, 0, vin)) || (st = dd_fields(dd, 1, vout)) || (st = dd_fields(dd, 2, t)) ||
+      (st = dd_fields(dd, 3, q)))
+    return st;
+  if ((st = dd_upload(dd, in, vin))) return st;
+  const bool w = which >= 3 && which <= 5;
+  OpParams op = op_of(p, w);
+  switch (which) {
+    case 0: case 3: st = dd_mtil(dd, false, vout, vin, t, op); break;
+    case 1: case 4: st = dd_mtil(dd, true, vout, vin, t, op); break;
+    case 2: case 5: st = dd_mdagm(dd, vout, vin, t, q, op); break;
+    default:  // 6: d(EVEN, ODD), 7: d_dag(EVEN, ODD)
+      if ((st = dd_exchange(dd, vin, which == 7))) break;
+      for (int s = 0; s < dd->nslabs(); s++)
+        launch_dd_dslash(dd->slabs[s]->g, dd->geom(s), 0, which == 7, vout[s], vin[s], dd->slabs[s]->gauge64,
+                         dd->stream);
+      st = cudaGetLastError() == cudaSuccess ? BQCDG_OK : BQCDG_ECUDA;
+  }
+  if (st) return st;
+  return dd_download(dd, vout, out);
+}
+
+// cg.F90:51-137 over the slabs: FP64, x the initial guess, absolute stop
+// rtr <= cgp->rest, (W^+W) with W = M~ + p->rho; the three scalars of each
+// iteration are global sums (cg.F90:91,97,109)
+int bqcdg_dd_cg(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p, const bqcdg_cg_para* cgp,
+                int* iterations, bqcdg_solve_info* info) {
+  int st = dd_check(dd);
+  if (st || !x || !b || !p || !cgp) return BQCDG_EINVAL;
+  for (bqcdg_ctx* c : dd->slabs) {
+    if (!c->have_gauge) return BQCDG_ENOGAUGE;
+    if (p->csw_kappa != 0.0 && (!c->have_A[0] || !c->have_Ainv[1])) return BQCDG_ENOCLOVER;
+  }
+  CK(cudaSetDevice(dd->slabs[0]->device));
+  bqcdg_solve_info tmp;
+  if (!info) info = &tmp;
+  std::memset(info, 0, sizeof(*info));
+  std::vector<double2*> vx, vb, vr, vp, vap, t, q;
+  if ((st = dd_fields(dd, 0, vx)) || (st = dd_fields(dd, 1, vb)) || (st = dd_fields(dd, 2, vr)) ||
+      (st = dd_fields(dd, 3, vp)) || (st = dd_fields(dd, 4, vap)) || (st = dd_fields(dd, 5, t)) ||
+      (st = dd_fields(dd, 6, q)))
+    return st;
+  if ((st = dd_upload(dd, x, vx)) || (st = dd_upload(dd, b, vb))) return st;
+  const OpParams op = op_of(p, true);
+  const int n = dd->nslabs();
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, dd->stream));
+  auto dot = [&](const std::vector<double2*>& a, const std::vector<double2*>& c2, double* out) {
+    for (int s = 0; s < n; s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_dot(c->g, a[s], c2[s], c->red, c->dres, dd->stream);
+    }
+    if (cudaGetLastError() != cudaSuccess) return BQCDG_ECUDA;
+    return dd_global_sum(dd, 1, out);
+  };
+  // r = b - A x, p = r
+  if ((st = dd_mdagm(dd, vr, vx, t, q, op))) return st;
+  for (int s = 0; s < n; s++) {
+    bqcdg_ctx* c = dd->slabs[s];
+    launch_caxpby(c->g, 1.0, 0.0, vb[s], -1.0, vr[s], dd->stream);  // r = b - r
+    CK(cudaMemcpyAsync(vp[s], vr[s], (size_t)12 * c->g.stride * sizeof(double2), cudaMemcpyDeviceToDevice,
+                       dd->stream));
+  }
+  CKL();
+  double rtrold = 0.0, rtr = 0.0, paap = 0.0;
+  if ((st = dot(vr, vr, &rtrold))) return st;
+  int niter = 0;
+  bool conv = false;
+  for (niter = 1; niter <= cgp->maxiter; niter++) {
+    if ((st = dd_mdagm(dd, vap, vp, t, q, op))) return st;
+    if ((st = dot(vp, vap, &paap))) return st;
+    const double ak = rtrold / paap;
+    for (int s = 0; s < n; s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_axpy(c->g, ak, vp[s], vx[s], dd->stream);
+      launch_axpy(c->g, -ak, vap[s], vr[s], dd->stream);
+    }
+    CKL();
+    if ((st = dot(vr, vr, &rtr))) return st;
+    if (!(rtr == rtr)) break;
+    if (rtr <= (double)cgp->rest) {
+      conv = true;
+      break;
+    }
+    const double bk = rtr / rtrold;
+    rtrold = rtr;
+    for (int s = 0; s < n; s++) launch_caxpby(dd->slabs[s]->g, 1.0, 0.0, vr[s], bk, vp[s], dd->stream);  // p = r + bk p
+    CKL();
+  }
+  if (!conv && niter > cgp->maxiter) niter = cgp->maxiter;
+  CK(cudaEventRecord(e1, dd->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if ((st = dd_download(dd, vx, x))) return st;
+  info->niter = niter;
+  info->rtr = rtr;
+  info->converged = conv ? 1 : 0;
+  info->seconds = ms * 1e-3;
+  if (iterations) *iterations = niter;
+  if (!(rtr == rtr)) return BQCDG_ENAN;
+  if (!conv && cgp->log != 2) return BQCDG_ENOCONV;
+  return BQCDG_OK;
+}
+
+}  // extern "C"

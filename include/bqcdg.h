@@ -328,6 +328,49 @@ int bqcdg_field_caxpby(bqcdg_ctx *ctx, int hy, double ay, double are, double aim
 #define BQCDG_MAX_DOT_PAIRS 8
 int bqcdg_field_cdot_pairs(bqcdg_ctx *ctx, int n, const int *ha, const int *hb, double *re, double *im);
 
+/* ---- domain decomposition in time ---------------------------------------- */
+/* The global lattice L is cut along t into nranks slabs of L[3]/nranks time
+ * slices (an even number, so a slab's parity is the global one).  Slab r
+ * holds the contiguous range [r V3h Lt, (r+1) V3h Lt) of BQCD's even/odd site
+ * index (V3h = L[0] L[1] L[2] / 2, Lt = L[3]/nranks).  Before each stencil
+ * pass every slab sends the two-spin half spinors that the t hop keeps
+ * (12 reals per site) of its first slice to rank-1 and of its last slice to
+ * rank+1, and the CG takes the global sums of its three scalars, as the
+ * reference's MPI build does (d/D21.F90:53-72, comm/xbound_mpi.F90:418-461,
+ * cg.F90:91,97,109).  U_t of each slab's last slice is sent to rank+1 once per
+ * gauge field.  Everything here is FP64.
+ *
+ * Two ways to run it:
+ *  - bqcdg_dd_create_local: all nranks slabs in this process on one device,
+ *    the faces copied between them on the device and the global sums added
+ *    on the host in rank order.  Host arrays are the GLOBAL ones.
+ *  - bqcdg_dd_create_nccl: one slab per process (rank `rank`, one GPU each),
+ *    faces by ncclSend/ncclRecv and sums by ncclAllReduce on the slab's
+ *    stream.  Rank 0 makes the id with bqcdg_dd_nccl_unique_id and hands its
+ *    128 bytes to the others (any side channel).  Host arrays are the slab's
+ *    own (volh = V3h Lt sites per parity).  libnccl.so.2 is opened at run
+ *    time; without it both calls return BQCDG_EUNSUPPORTED. */
+typedef struct bqcdg_dd bqcdg_dd;
+int bqcdg_dd_create_local(bqcdg_dd **dd, const int L[4], const int bc[4], int nranks, int device);
+int bqcdg_dd_nccl_unique_id(char *id128);
+int bqcdg_dd_create_nccl(bqcdg_dd **dd, const int L[4], const int bc[4], int nranks, int rank, int device,
+                         const char *id128);
+int bqcdg_dd_destroy(bqcdg_dd *dd);
+/* sites per parity of the host spinors this process passes */
+int bqcdg_dd_volh(const bqcdg_dd *dd);
+/* conf%u (flipped = 1: flip_bc applied, whose sign is on the global last
+ * slice only) and conf%a, conf%i of both parities (CLOVER_FIELD_A layout) */
+int bqcdg_dd_load_gauge(bqcdg_dd *dd, const double *u, int flipped);
+int bqcdg_dd_load_clover(bqcdg_dd *dd, const double *a, const double *ainv);
+/* out = op(in) on even-site spinors: which = 0 mtil, 1 mtil_dag, 2 mtdagmt,
+ * 3 w_mult, 4 w_mult_dag, 5 w_dagger_w (as bqcdg_op_dev), 6 d(EVEN, ODD) and
+ * 7 d_dag(EVEN, ODD) (in: odd sites) */
+int bqcdg_dd_op(bqcdg_dd *dd, int which, double *out, const double *in, const bqcdg_params *p);
+/* cg(matrix_mult, x, b, ...) (cg.F90:51-137) on the decomposed lattice:
+ * FP64, x the initial guess, |r|^2 <= cgp->rest, W = M~ + p->rho */
+int bqcdg_dd_cg(bqcdg_dd *dd, double *x, const double *b, const bqcdg_params *p, const bqcdg_cg_para *cgp,
+                int *iterations, bqcdg_solve_info *info);
+
 /* ---- allocation-free operator ------------------------------------------- */
 /* This entry point has no counterpart in the reference.  It is for callers
  * that cannot let the library allocate device memory: a framework whose pool

@@ -98,3 +98,14 @@ def test_noalloc_argument_and_size_checks(so, bq):
     assert f((C.c_int * 4)(5, 4, 4, 4), bc, one, one, one, C.byref(prm), one, one, None) == bq.EINVAL
     clov = bq.Params(0.13, 0.25, 0.0, 0.0)  # csw != 0 needs both clover parts
     assert f(small, bc, one, None, one, C.byref(clov), one, one, None) == bq.ENOCLOVER
+
+
+def test_slab_decomposition_shape_is_checked(bq):
+    """bqcdg_dd_create_local refuses slabs that do not divide the time
+    extent into an even number of slices each, before it touches a device."""
+    with pytest.raises(bq.BqcdgError) as e:
+        bq.SlabDecomposition.local((8, 8, 8, 8), 3)        # 8 slices do not split into 3
+    assert e.value.status == bq.EINVAL
+    with pytest.raises(bq.BqcdgError) as e:
+        bq.SlabDecomposition.local((8, 8, 8, 12), 4)       # slabs of 3 slices would mix parities
+    assert e.value.status == bq.EINVAL
