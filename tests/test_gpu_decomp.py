@@ -37,11 +37,11 @@ def setup(request, oracle, bq):
 
 
 @pytest.mark.parametrize("dag", [False, True])
-def test_decomposed_dslash(setup, dag):
+def test_decomposed_dslash(setup, bq, dag):
     g, dd = setup["g"], setup["dd"]
     psi = g.gauss_spinor(1)
     ref = g.d(0, 1, psi, setup["uf"], dag)
-    got = dd.op("d_dag" if dag else "d", psi, None)
+    got = dd.op("d_dag" if dag else "d", psi, bq.HmcPara(kappa=setup["kappa"]))
     assert rel(got, ref) < 1e-13
 
 
