@@ -98,6 +98,9 @@ def _lib_handle():
         L.bqcdg_load_clover_solver.argtypes = [vp, dp, dp]
         L.bqcdg_clover_init.argtypes = [vp, C.c_double]
         L.bqcdg_clover_init_solver.argtypes = [vp, C.c_double]
+        L.bqcdg_clover_init_t.argtypes = [vp, C.c_double]
+        L.bqcdg_solve_batch_kappa.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, dp, dp,
+                                              P(SolverOpts), i, P(SolveInfo)]
         L.bqcdg_release_scratch.argtypes = [vp, i]
         L.bqcdg_conf_write.argtypes = [vp, C.c_char_p, P(ConfMeta)]
         L.bqcdg_conf_read.argtypes = [vp, C.c_char_p, P(ConfMeta)]
@@ -599,6 +602,32 @@ class Lattice:
                                              r.ctypes.data, tols.ctypes.data, C.byref(o), block, infos)
         if st not in (OK, ENOCONV):
             _check(st, "solve_batch_shifted")
+        return list(infos)
+
+    def clover_init_t(self, csw):
+        """The clover term for any kappa (bqcdg_clover_init_t): operators
+        then build A(kappa) = 1 + kappa T at the kappa of their parameters."""
+        _check(lib().bqcdg_clover_init_t(self.h, csw), "clover_init_t")
+
+    def solve_batch_kappa(self, hxs, hbs, para, kappas, rhos=None, precision=PREC_HALF, tol=1e-10, relative=True,
+                          maxiter=100000, delta=0.1, block=0):
+        """Batched solve of (W_k^+W_k) x_k = b_k, W_k = M~(kappa_k) + rho_k:
+        each system its own hopping parameter (and clover term, from
+        clover_init_t) and shift; para gives c_sw (nonzero: clover) and h."""
+        n = len(hxs)
+        if len(kappas) != n or len(hbs) != n or (rhos is not None and len(rhos) != n):
+            raise ValueError("solve_batch_kappa: one b, one kappa (and one rho) per x")
+        tols = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, dtype=np.float64), (n,)))
+        o = SolverOpts(precision, maxiter, int(relative), float(tols[0]), delta, 1, 0, 1)
+        infos = (SolveInfo * n)()
+        prm = para.params(0.0) if isinstance(para, HmcPara) else para
+        k = np.ascontiguousarray(kappas, dtype=np.float64)
+        r = None if rhos is None else np.ascontiguousarray(rhos, dtype=np.float64)
+        st = lib().bqcdg_solve_batch_kappa(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm),
+                                           k.ctypes.data, None if r is None else r.ctypes.data, tols.ctypes.data,
+                                           C.byref(o), block, infos)
+        if st not in (OK, ENOCONV):
+            _check(st, "solve_batch_kappa")
         return list(infos)
 
     def mdagm_dev(self, hout, hin, para, precision, n, rho=None):

@@ -134,6 +134,7 @@ struct Geom {
   int bcsign[4];   // fermion boundary sign per direction (+1 / -1)
   int rec12;       // FP64 stencil links stored as 12 reals (columns 1,2)
   FastDiv dxh, d1, d2;  // division by Lxh, L[1], L[2] (geom_finish)
+  int clover_t;    // the clover fields hold T, with A(kappa) = 1 + kappa T (clover_apply_kt)
 };
 // fills the derived members once L and Lxh are set
 inline void geom_finish(Geom& g) {
@@ -694,6 +695,117 @@ __device__ __forceinline__ void clover_apply(const CloverView<P>& A, int i, cons
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) out.c[a][b] = sc * out.c[a][b];
+}
+
+// ---------------------------------------------------------------------------
+// clover blocks at any hopping parameter.  clover_init.F90:46-77 builds each
+// chiral block as 1 + (-c_sw kappa / 8)(p +- q), from field strengths that
+// do not depend on kappa; with T = (-c_sw / 8)(p +- q) stored in the packed
+// slots in place of the block, A(kappa) = 1 + kappa T gives every kappa its
+// own clover term from one field.  The stored blocks of BQCD are halved
+// (clover_inv.F90:105-137, 211-216): a = A/2, ainv = A^-1 / 2.
+// ---------------------------------------------------------------------------
+// out = (A(kappa) / 2) in on one site, in the chiral layout of clover_apply_raw
+template <typename CV, typename R>
+__device__ __forceinline__ void clover_apply_kt(const CV& T, int i, const Spinor<R>& in, Spinor<R>& out, R kappa) {
+  cx<R> x[6], y[6], a[18];
+  R sc;
+#pragma unroll
+  for (int chi = 0; chi < 2; chi++) {
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      x[k] = chi == 0 ? in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3] : in.c[k / 3][k % 3] - in.c[k / 3 + 2][k % 3];
+    T.load_block_raw(i, chi, a, sc);
+    clover_block_mv(a, x, y);
+    const R hk = R(0.5) * kappa * sc;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const cx<R> z = mkc(fma(hk, y[k].x, R(0.5) * x[k].x), fma(hk, y[k].y, R(0.5) * x[k].y));
+      if (chi == 0) {
+        out.c[k / 3][k % 3] = z;
+        out.c[k / 3 + 2][k % 3] = z;
+      } else {
+        out.c[k / 3][k % 3] = out.c[k / 3][k % 3] + z;
+        out.c[k / 3 + 2][k % 3] = out.c[k / 3 + 2][k % 3] - z;
+      }
+    }
+  }
+}
+
+// y = (A(kappa)^-1 / 2) x for one packed block a (raw values times sc): the
+// LDL^+ factorisation of clover_inv.F90:45-101 in registers, then the
+// substitutions of clover_mult_b.h90
+template <typename R>
+__device__ __forceinline__ void block_inv_apply_kt(const cx<R> a[18], R sc, R kappa, const cx<R> x[6], cx<R> y[6]) {
+  // packed upper-triangle slot of (r, c), r < c (clover.h:28-55)
+  constexpr int up[6][6] = {{-1, 1, 2, 3, 4, 5},    {-1, -1, 6, 7, 8, 9},    {-1, -1, -1, 11, 12, 13},
+                            {-1, -1, -1, -1, 14, 15}, {-1, -1, -1, -1, -1, 17}, {-1, -1, -1, -1, -1, -1}};
+  const R ks = kappa * sc;
+  R dg[6];
+  dg[0] = a[0].x; dg[1] = a[0].y; dg[2] = a[10].x; dg[3] = a[10].y; dg[4] = a[16].x; dg[5] = a[16].y;
+  cx<R> L[6][6];
+  R d[6], dinv[6];
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    cx<R> tmp[6];
+#pragma unroll
+    for (int c = 0; c < r; c++) {
+      cx<R> t = ks * conjg(a[up[c][r]]);  // A(r, c) = conj(A(c, r))
+#pragma unroll
+      for (int k = 0; k < c; k++) t = t - tmp[k] * conjg(L[c][k]);
+      tmp[c] = t;
+    }
+#pragma unroll
+    for (int c = 0; c < r; c++) L[r][c] = dinv[c] * tmp[c];
+    R dr = R(1) + ks * dg[r];
+#pragma unroll
+    for (int k = 0; k < r; k++) dr = dr - d[k] * norm2(L[r][k]);
+    d[r] = dr;
+    dinv[r] = R(1) / dr;
+  }
+  cx<R> w[6];
+#pragma unroll
+  for (int r = 0; r < 6; r++) {
+    cx<R> t = x[r];
+#pragma unroll
+    for (int c = 0; c < r; c++) t = t - L[r][c] * w[c];
+    w[r] = t;
+  }
+#pragma unroll
+  for (int r = 5; r >= 0; r--) {
+    cx<R> t = dinv[r] * w[r];
+#pragma unroll
+    for (int c = r + 1; c < 6; c++) t = t - conjg(L[c][r]) * y[c];
+    y[r] = t;
+  }
+#pragma unroll
+  for (int r = 0; r < 6; r++) y[r] = R(0.5) * y[r];
+}
+
+// out = (A(kappa)^-1 / 2) in on one site
+template <typename CV, typename R>
+__device__ __forceinline__ void clover_inv_apply_kt(const CV& T, int i, const Spinor<R>& in, Spinor<R>& out,
+                                                    R kappa) {
+  cx<R> x[6], y[6], a[18];
+  R sc;
+#pragma unroll
+  for (int chi = 0; chi < 2; chi++) {
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      x[k] = chi == 0 ? in.c[k / 3][k % 3] + in.c[k / 3 + 2][k % 3] : in.c[k / 3][k % 3] - in.c[k / 3 + 2][k % 3];
+    T.load_block_raw(i, chi, a, sc);
+    block_inv_apply_kt(a, sc, kappa, x, y);
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      if (chi == 0) {
+        out.c[k / 3][k % 3] = y[k];
+        out.c[k / 3 + 2][k % 3] = y[k];
+      } else {
+        out.c[k / 3][k % 3] = out.c[k / 3][k % 3] + y[k];
+        out.c[k / 3 + 2][k % 3] = out.c[k / 3 + 2][k % 3] - y[k];
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -414,23 +414,36 @@ int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* 
 // per stencil thread (2, 4: the register-blocked passes of dslash_multi.cu;
 // 0: timed choice).
 int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op, Prec sloppy, int maxiter,
-             const double* stop, double delta, bqcdg_solve_info* info, const double* rho, int nbt) {
+             const double* stop, double delta, bqcdg_solve_info* info, const double* rho, int nbt,
+             const double* kappa) {
   const Geom& g = c->g;
   int st = ensure_sloppy(c, sloppy, op.csw_kappa != 0.0);
   if (st) return st;
   if ((st = ensure_batch(c, sloppy, nb))) return st;
   auto& B = c->batch;
-  if (nbt == 0 && (st = tune_nbt(c, sloppy, op, nb, &nbt))) return st;
-  if (nbt > nb || op.h != 0.0) nbt = 1;  // the register-blocked passes take h = 0 only
-  // the operator of right-hand side k: op, with its own shift when rho is given
+  // the register-blocked passes take h = 0, one kappa and the stored clover
+  // blocks only
+  const bool blocked_ok = op.h == 0.0 && !kappa && !g.clover_t;
+  if (nbt == 0 && blocked_ok && (st = tune_nbt(c, sloppy, op, nb, &nbt))) return st;
+  if (nbt > nb || !blocked_ok) nbt = 1;
+  // the operator of right-hand side k: op, with its own shift when rho is
+  // given and its own hopping parameter when kappa is
   std::vector<OpParams> ops(nb, op);
   const double* drho = nullptr;
+  const double* dkap = nullptr;
   if (rho) {
     for (int k = 0; k < nb; k++) ops[k].rho = rho[k];
     std::memcpy(c->hres, rho, sizeof(double) * nb);
     CK(cudaMemcpyAsync(c->drho, c->hres, sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));  // hres is reused below
     drho = c->drho;
+  }
+  if (kappa) {
+    for (int k = 0; k < nb; k++) ops[k].kappa = kappa[k];
+    std::memcpy(c->hres, kappa, sizeof(double) * nb);
+    CK(cudaMemcpyAsync(c->dkappa, c->hres, sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    dkap = c->dkappa;
   }
   CK(cudaEventRecord(c->ev0, c->stream));
   std::vector<int> ru(nb, 0), fin(nb, 0), conv(nb, 0), nl(nb, 0), stall(nb, 0), stalled(nb, 0);
@@ -476,13 +489,13 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
                           c->dcg, c->stream, nb, drho, nbt);
       } else {
         launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
-                          c->stream, nb);
+                          c->stream, nb, dkap);
         launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red,
-                          nullptr, c->dcg, c->stream, nb, drho);
+                          nullptr, c->dcg, c->stream, nb, drho, dkap);
         launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
-                          c->stream, nb);
+                          c->stream, nb, dkap);
         launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
-                        c->dcg, c->stream, nb, true, drho);
+                        c->dcg, c->stream, nb, true, drho, dkap);
       }
       launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
     }
@@ -602,7 +615,7 @@ int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* 
   float best = 0.f;
   int choice = 1;
   for (int k : {1, 2, 4}) {
-    if (k > 1 && (k > nb || op.h != 0.0 || p == Prec::F64)) break;
+    if (k > 1 && (k > nb || op.h != 0.0 || p == Prec::F64 || c->g.clover_t)) break;
     float t;
     int st = time_pass1(c, p, op, nb, k, 3, &t);
     if (st) return st;
@@ -705,6 +718,7 @@ int bqcdg_create(bqcdg_ctx** out, const int L[4], const int bc[4], int device) {
   if (e == cudaSuccess) e = cudaMemsetAsync(c->red.counter, 0, sizeof(unsigned int) * kMaxRhs, c->stream);
   if (e == cudaSuccess) e = c->alloc((void**)&c->dres, sizeof(double) * 16);
   if (e == cudaSuccess) e = c->alloc((void**)&c->drho, sizeof(double) * kMaxRhs);
+  if (e == cudaSuccess) e = c->alloc((void**)&c->dkappa, sizeof(double) * kMaxRhs);
   if (e == cudaSuccess) e = c->alloc((void**)&c->dcg, sizeof(CgScalars) * kMaxRhs);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hres, sizeof(double) * 16);
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->hcg, sizeof(CgScalars) * kMaxRhs);
@@ -806,6 +820,34 @@ int bqcdg_get_gauge(bqcdg_ctx* c, double* u, int flipped) {
   return BQCDG_OK;
 }
 
+// the clover term at any kappa: T = (-c_sw / 8)(p +- q) of the even sites in
+// A[0] and of the odd sites in Ainv[1], the two fields the even-odd
+// operator reads; the kernels form A(kappa) = 1 + kappa T and its inverse per
+// site (g.clover_t)
+static int clover_init_t(bqcdg_ctx* c, double csw) {
+  if (!c->have_gauge) return BQCDG_ENOGAUGE;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  double2** unused[4] = {&c->A[1], &c->Ainv[0], &c->B[0], &c->B[1]};
+  for (double2** f : unused) {
+    c->release(*f);
+    *f = nullptr;
+  }
+  const size_t n = (size_t)36 * c->g.stride * sizeof(double2);
+  if (!c->A[0]) CK(c->alloc((void**)&c->A[0], n));
+  if (!c->Ainv[1]) CK(c->alloc((void**)&c->Ainv[1], n));
+  if (!c->clov_tmp) CK(c->alloc((void**)&c->clov_tmp, (size_t)54 * clover_init_chunk(c->g) * sizeof(double2)));
+  double2* t[2] = {c->A[0], c->Ainv[1]};
+  launch_clover_t(c->g, c->gauge64, csw, t, c->clov_tmp, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  for (int eo = 0; eo < 2; eo++) c->have_A[eo] = c->have_Ainv[eo] = c->have_B[eo] = false;
+  c->have_A[0] = c->have_Ainv[1] = true;
+  for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  c->g.clover_t = c->g12.clover_t = 1;
+  return BQCDG_OK;
+}
+
 // the parities eo0..eo1 of one clover field from its Fortran array
 static int load_clover_field(bqcdg_ctx* c, double2** dst, bool* have, const double* src, int eo0 = 0,
                              int eo1 = 1) {
@@ -838,6 +880,7 @@ int bqcdg_load_clover(bqcdg_ctx* c, const double* a, const double* ainv, const d
     }
   }
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  c->g.clover_t = c->g12.clover_t = 0;
   CK(cudaStreamSynchronize(c->stream));
   return BQCDG_OK;
 }
@@ -858,6 +901,7 @@ int bqcdg_load_clover_solver(bqcdg_ctx* c, const double* a, const double* ainv) 
   if ((st = load_clover_field(c, c->A, c->have_A, a, 0, 0))) return st;
   if ((st = load_clover_field(c, c->Ainv, c->have_Ainv, ainv, 1, 1))) return st;
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  c->g.clover_t = c->g12.clover_t = 0;
   CK(cudaStreamSynchronize(c->stream));
   return BQCDG_OK;
 }
@@ -876,6 +920,8 @@ static int get_clover_field(bqcdg_ctx* c, double2** srcs, const bool* have, doub
 }
 
 int bqcdg_get_clover(bqcdg_ctx* c, double* a, double* ainv, double* b) {
+  // the fields hold T (bqcdg_clover_init_t), not BQCD's blocks
+  if (c && c->g.clover_t) return BQCDG_EUNSUPPORTED;
   if (!c) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   int st;
@@ -901,6 +947,7 @@ int bqcdg_clover_init(bqcdg_ctx* c, double csw_kappa) {
   CK(cudaStreamSynchronize(c->stream));
   for (int eo = 0; eo < 2; eo++) c->have_A[eo] = c->have_Ainv[eo] = c->have_B[eo] = true;
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  c->g.clover_t = c->g12.clover_t = 0;
   return BQCDG_OK;
 }
 
@@ -928,6 +975,7 @@ int bqcdg_clover_init_solver(bqcdg_ctx* c, double csw_kappa) {
   c->have_A[0] = c->have_Ainv[1] = true;
   c->have_A[1] = c->have_Ainv[0] = c->have_B[0] = c->have_B[1] = false;
   for (int k = 0; k < 3; k++) c->clover_s_ok[k] = false;
+  c->g.clover_t = c->g12.clover_t = 0;
   return BQCDG_OK;
 }
 
@@ -963,6 +1011,8 @@ int bqcdg_d_dag(bqcdg_ctx* c, int e, int o, double* out, const double* in) {
 }
 
 static int clover_host(bqcdg_ctx* c, int eo, double* out, const double* in, int which) {
+  // the fields hold T (bqcdg_clover_init_t), not BQCD's blocks
+  if (c && c->g.clover_t) return BQCDG_EUNSUPPORTED;
   if (!c || !out || !in || eo < 0 || eo > 1) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
   double2* si = c->sp64(0);
@@ -1163,6 +1213,8 @@ extern "C" {
 
 namespace bqcdg_host {
 int dsf_core(bqcdg_ctx* c, double* p, double step, const bqcdg_params* par, double2* da, double2* db) {
+  // the fields hold T (bqcdg_clover_init_t), not BQCD's blocks
+  if (c && c->g.clover_t) return BQCDG_EUNSUPPORTED;
   int st = ensure_force_bufs(c);
   if (st) return st;
   double2 *dat = c->sp64(2), *dbt = c->sp64(3);
@@ -1247,6 +1299,8 @@ int bqcdg_clover_dsf(bqcdg_ctx* c, int eo, double* p, const double* b, const dou
 
 namespace bqcdg_host {
 int dsd_core(bqcdg_ctx* c, double* p, int eo, double s) {
+  // the fields hold T (bqcdg_clover_init_t), not BQCD's blocks
+  if (c && c->g.clover_t) return BQCDG_EUNSUPPORTED;
   launch_clover_ts(c->g, c->wbuf, c->Ainv[eo], c->stream);
   launch_clover_d(c->g, p, c->gauge64, c->wbuf, eo, s, c->stream);
   CKL();
@@ -1423,7 +1477,7 @@ int bqcdg_solve_dev(bqcdg_ctx* c, int hx, int hb, const bqcdg_params* p, const b
 // tolerance per right-hand side (null: o->tol for all)
 static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
                        const double* rho, const double* tol, const bqcdg_solver_opts* o, int block,
-                       bqcdg_solve_info* infos) {
+                       bqcdg_solve_info* infos, const double* kappa = nullptr) {
   int st = check_op(c, p);
   if (st) return st;
   if (!o || !hx || !hb || !infos || nrhs <= 0 || block < 0 || block > kMaxRhs) return BQCDG_EINVAL;
@@ -1435,6 +1489,11 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
   if (tol)
     for (int k = 0; k < nrhs; k++)
       if (!(tol[k] >= 0.0)) return BQCDG_EINVAL;
+  if (kappa)
+    for (int k = 0; k < nrhs; k++)
+      if (!(kappa[k] > 0.0)) return BQCDG_EINVAL;
+  // kappa per right-hand side with the clover term needs T (bqcdg_clover_init_t)
+  if (kappa && p->csw_kappa != 0.0 && !c->g.clover_t) return BQCDG_ENOCLOVER;
   for (int k = 0; k < nrhs; k++)
     if (!field(c, hx[k]) || !field(c, hb[k])) return BQCDG_EINVAL;
   CK(cudaSetDevice(c->device));
@@ -1469,13 +1528,14 @@ static int solve_batch(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, con
       bs[k] = field(c, hb[k0 + k]);
     }
     st = cg_batch(c, xs.data(), bs.data(), nb, op, sl, o->maxiter, stop.data() + k0, o->delta, infos + k0,
-                  rho ? rho + k0 : nullptr, o->rhs_per_thread);
+                  rho ? rho + k0 : nullptr, o->rhs_per_thread, kappa ? kappa + k0 : nullptr);
     if (st) return st;
     for (int k = 0; k < nb; k++) {
       bqcdg_solve_info& in = infos[k0 + k];
       if (o->check_true_residual) {
         OpParams opk = op;
         if (rho) opk.rho = rho[k0 + k];
+        if (kappa) opk.kappa = kappa[k0 + k];
         if ((st = true_residual(c, xs[k], bs[k], opk, &in.true_rtr))) return st;
         in.converged = in.true_rtr <= stop[k0 + k] ? 1 : 0;
       }
@@ -1495,6 +1555,18 @@ int bqcdg_solve_batch_shifted(bqcdg_ctx* c, int nrhs, const int* hx, const int* 
                               bqcdg_solve_info* infos) {
   if (!rho) return BQCDG_EINVAL;
   return solve_batch(c, nrhs, hx, hb, p, rho, tol, o, block, infos);
+}
+
+int bqcdg_solve_batch_kappa(bqcdg_ctx* c, int nrhs, const int* hx, const int* hb, const bqcdg_params* p,
+                            const double* kappa, const double* rho, const double* tol, const bqcdg_solver_opts* o,
+                            int block, bqcdg_solve_info* infos) {
+  if (!kappa) return BQCDG_EINVAL;
+  return solve_batch(c, nrhs, hx, hb, p, rho, tol, o, block, infos, kappa);
+}
+
+int bqcdg_clover_init_t(bqcdg_ctx* c, double csw) {
+  if (!c) return BQCDG_EINVAL;
+  return clover_init_t(c, csw);
 }
 
 int bqcdg_mdagm_dev(bqcdg_ctx* c, int hout, int hin, const bqcdg_params* p, int precision, int n, double* ms) {

@@ -206,8 +206,9 @@ __device__ __forceinline__ void load_plane(const double2* tmp, int n, int k, int
 
 // clover_init3 (a1 = s(p+q)+1, a2 = s(p-q)+1, upper triangle) and
 // clover_inv for chiral block chi = blockIdx.y of each site
+// tmode: store T = factor (p +- q) itself (no identity, not halved, no inverse)
 __global__ void __launch_bounds__(64) k_clover_blocks(Geom g, const double2* tmp, int i0, int n, double factor,
-                                                      double2* A, double2* AI, double2* B) {
+                                                      double2* A, double2* AI, double2* B, int tmode) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int chi = blockIdx.y;
   if (k >= n) return;
@@ -226,6 +227,10 @@ __global__ void __launch_bounds__(64) k_clover_blocks(Geom g, const double2* tmp
   const double sg = chi == 0 ? 1.0 : -1.0;
   for (int r = 0; r < 6; r++)
     for (int c = r; c < 6; c++) bl.m[r][c] = factor * (p.m[r][c] + sg * q.m[r][c]);
+  if (tmode) {
+    store_packed(A, g.stride, i0 + k, chi, bl, 1.0);
+    return;
+  }
   for (int r = 0; r < 6; r++) bl.m[r][r] = mkc(bl.m[r][r].x + 1.0, 0.0);
   block_inv(bl, A, AI, B, g.stride, i0 + k, chi);
 }
@@ -241,7 +246,19 @@ void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, d
       const int n = g.volh - i0 < chunk ? g.volh - i0 : chunk;
       k_clover_fields<<<dim3((n + 63) / 64, 6), 64, 0, s>>>(g, gauge, eo, i0, n, tmp);
       k_clover_blocks<<<dim3((n + 63) / 64, 2), 64, 0, s>>>(g, tmp, i0, n, -csw_kappa / 8.0, a[eo], ainv[eo],
-                                                            b[eo]);
+                                                            b[eo], 0);
+    }
+  }
+}
+
+void launch_clover_t(const Geom& g, const double2* gauge, double csw, double2* t[2], double2* tmp, cudaStream_t s) {
+  const int chunk = clover_init_chunk(g);
+  for (int eo = 0; eo < 2; eo++) {
+    if (!t[eo]) continue;
+    for (int i0 = 0; i0 < g.volh; i0 += chunk) {
+      const int n = g.volh - i0 < chunk ? g.volh - i0 : chunk;
+      k_clover_fields<<<dim3((n + 63) / 64, 6), 64, 0, s>>>(g, gauge, eo, i0, n, tmp);
+      k_clover_blocks<<<dim3((n + 63) / 64, 2), 64, 0, s>>>(g, tmp, i0, n, -csw / 8.0, t[eo], nullptr, nullptr, 1);
     }
   }
 }

@@ -59,6 +59,7 @@ struct bqcdg_ctx {
   double* dres = nullptr;        // device result scalars [16]
   double* hres = nullptr;        // pinned mirror
   double* drho = nullptr;        // per right-hand-side shifts of a batch [kMaxRhs]
+  double* dkappa = nullptr;      // per right-hand-side hopping parameters of a batch [kMaxRhs]
   CgScalars* dcg = nullptr;
   CgScalars* hcg = nullptr;      // pinned
 

@@ -159,10 +159,13 @@ void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStrea
 // mtil / mtil_dag, first half (m_tilde.F90:55-58, 92-95):
 //   t_o = Ainv_oo D_oe in_e, then (1 - i h g5) t_o for mtil, (1 + i h g5) for mtil_dag
 // ---------------------------------------------------------------------------
-template <Prec P, bool DAG>
+// KT: the clover field holds T (clover_apply_kt), A(kappa)^-1 is formed per
+// site at kappa, or at kappa_rhs[rhs] (one hopping parameter per right-hand
+// side) when that is given
+template <Prec P, bool DAG, bool KT>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge,
                                                   CloverPtr ainv, int has_clover, double hval, const CgScalars* cg,
-                                                  int nr) {
+                                                  int nr, double kappa, const double* kappa_rhs) {
   using R = typename SpinorView<P>::R;
   const Tile tl = tile(nr);
   if (cg && cg[tl.rhs].done) return;  // retired right-hand side
@@ -179,7 +182,8 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
   R osc = 1;  // a common factor of the output, folded into its storage scale
   if (has_clover) {
     Spinor<R> y;
-    clover_apply_raw(cview<P>(ainv, g.stride), i, b, y, osc);
+    if constexpr (KT) clover_inv_apply_kt(cview<P>(ainv, g.stride), i, b, y, (R)(kappa_rhs ? kappa_rhs[tl.rhs] : kappa));
+    else clover_apply_raw(cview<P>(ainv, g.stride), i, b, y, osc);
     b = y;
   }
   if (hval != 0.0) h_mult_b(b, (R)hval);
@@ -187,14 +191,18 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
 }
 
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
-                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr) {
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr,
+                       const double* kappa_rhs) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double hv = dag ? op.h : -op.h;
-#define P1(PP, D) k_pass1<PP, D><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr)
-  if (p == Prec::F64) { if (dag) P1(Prec::F64, true); else P1(Prec::F64, false); }
-  else if (p == Prec::F32) { if (dag) P1(Prec::F32, true); else P1(Prec::F32, false); }
-  else { if (dag) P1(Prec::F16, true); else P1(Prec::F16, false); }
+#define P1(PP, D, K) \
+  k_pass1<PP, D, K><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr, op.kappa, kappa_rhs)
+#define P1K(PP, D) if (g.clover_t) P1(PP, D, true); else P1(PP, D, false);
+  if (p == Prec::F64) { if (dag) { P1K(Prec::F64, true) } else { P1K(Prec::F64, false) } }
+  else if (p == Prec::F32) { if (dag) { P1K(Prec::F32, true) } else { P1K(Prec::F32, false) } }
+  else { if (dag) { P1K(Prec::F16, true) } else { P1K(Prec::F16, false) } }
+#undef P1K
 #undef P1
 }
 
@@ -204,18 +212,20 @@ void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorP
 // onto them, so the clover block and x are dead before the neighbour gathers
 // start; b is applied inside the hop sum and the storage scales of x and A_ee
 // as one factor, so no field is rescaled component by component.
-template <Prec P, bool DAG>
+template <Prec P, bool DAG, bool KT>
 __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorView<P>& t, const SpinorView<P>& xin,
                                            const GaugeView<P>& U, const CloverPtr& aee, int has_clover, double bcoef,
-                                           double hval, double rho, Spinor<typename SpinorView<P>::R>& out) {
+                                           double hval, double rho, Spinor<typename SpinorView<P>::R>& out,
+                                           double kappa) {
   using R = typename SpinorView<P>::R;
   Spinor<R> x;
   R xsc;
   xin.load_raw(i, x, xsc);
   const R rr = (R)rho * xsc;
   if (has_clover) {
-    R csc;
-    clover_apply_raw(cview<P>(aee, g.stride), i, x, out, csc);
+    R csc = 1;
+    if constexpr (KT) clover_apply_kt(cview<P>(aee, g.stride), i, x, out, (R)kappa);
+    else clover_apply_raw(cview<P>(aee, g.stride), i, x, out, csc);
     const R k = csc * xsc;
 #pragma unroll
     for (int s = 0; s < 4; s++)
@@ -243,15 +253,20 @@ __device__ __forceinline__ void pass2_core(const Geom& g, int i, const SpinorVie
   else wilson_hop<P, DAG>(g, 0, i, st, t, U, out, (R)bcoef);
 }
 
-template <Prec P, bool DAG, bool REDUCE>
+template <Prec P, bool DAG, bool REDUCE, bool KT>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp,
                                                   const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                                                   double hval, double rho, RedScratch red, double* norm_out,
-                                                  CgScalars* cg, int nr, const double* rho_rhs) {
+                                                  CgScalars* cg, int nr, const double* rho_rhs, double kappa,
+                                                  const double* kappa_rhs) {
   using R = typename SpinorView<P>::R;
   const Tile tl = tile(nr);
   if (cg && cg[tl.rhs].done) return;  // retired right-hand side
   if (rho_rhs) rho = rho_rhs[tl.rhs];   // a shift per right-hand side
+  if (kappa_rhs) {                       // a hopping parameter per right-hand side
+    kappa = kappa_rhs[tl.rhs];
+    bcoef = -kappa * kappa / (1.0 + hval * hval);
+  }
   const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
@@ -260,7 +275,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
     auto out = sview<P>(rhs_of(outp, tl.rhs), g.stride);
     auto U = gview<P>(gauge, g);
     Spinor<R> o;
-    pass2_core<P, DAG>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o);
+    pass2_core<P, DAG, KT>(g, i, t, xin, U, aee, has_clover, bcoef, hval, rho, o, kappa);
     out.store(i, o);
     if (REDUCE) {
 #pragma unroll
@@ -290,17 +305,21 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
 
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s, int nr, const double* rho_rhs) {
+                       CgScalars* cg, cudaStream_t s, int nr, const double* rho_rhs, const double* kappa_rhs) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = dag ? -op.h : op.h;
   bool reduce = norm_out != nullptr || cg != nullptr;
-#define P2(PP, D, RR)                                                                                                \
-  k_pass2<PP, D, RR><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, norm_out, \
-                                             cg, nr, rho_rhs)
-#define P2R(PP, D) \
-  if (reduce) P2(PP, D, true); else P2(PP, D, false);
+#define P2(PP, D, RR, K)                                                                                        \
+  k_pass2<PP, D, RR, K><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, \
+                                                norm_out, cg, nr, rho_rhs, op.kappa, kappa_rhs)
+#define P2R(PP, D)                                         \
+  if (g.clover_t) {                                        \
+    if (reduce) P2(PP, D, true, true); else P2(PP, D, false, true);   \
+  } else {                                                 \
+    if (reduce) P2(PP, D, true, false); else P2(PP, D, false, false); \
+  }
   if (p == Prec::F64) { if (dag) { P2R(Prec::F64, true) } else { P2R(Prec::F64, false) } }
   else if (p == Prec::F32) { if (dag) { P2R(Prec::F32, true) } else { P2R(Prec::F32, false) } }
   else { if (dag) { P2R(Prec::F16, true) } else { P2R(Prec::F16, false) } }
@@ -322,17 +341,22 @@ struct XR<Prec::F32> {
   using View = SpinorView<Prec::F32>;
 };
 
-template <Prec P, Prec XP, bool XUPD>
+template <Prec P, Prec XP, bool XUPD, bool KT>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge,
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
-                                                     RedScratch red, CgScalars* cgs, int nr, const double* rho_rhs) {
+                                                     RedScratch red, CgScalars* cgs, int nr, const double* rho_rhs,
+                                                     double kappa, const double* kappa_rhs) {
   using R = typename SpinorView<P>::R;
   using RX = typename SpinorView<XP>::R;
   const Tile tl = tile(nr);
   CgScalars* cg = cgs + tl.rhs;
   if (cg->done) return;  // retired right-hand side
   if (rho_rhs) rho = rho_rhs[tl.rhs];  // a shift per right-hand side
+  if (kappa_rhs) {                      // a hopping parameter per right-hand side
+    kappa = kappa_rhs[tl.rhs];
+    bcoef = -kappa * kappa / (1.0 + hval * hval);
+  }
   const int i = tl.i;
   double acc[1] = {0.0};
   if (i < g.volh) {
@@ -360,7 +384,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
       xv.store(i, xl);
     }
     Spinor<R> ap;
-    pass2_core<P, true>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap);
+    pass2_core<P, true, KT>(g, i, t, q, U, aee, has_clover, bcoef, hval, rho, ap, kappa);
     Spinor<RX> rl;
     rv.load(i, rl);
 #pragma unroll
@@ -386,17 +410,19 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
 
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr, bool xupd, const double* rho_rhs) {
+                     cudaStream_t s, int nr, bool xupd, const double* rho_rhs, const double* kappa_rhs) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = -op.h;  // mtil_dag
-#define P4(PP, XX, XU)                                                                                          \
-  k_cg_pass4<PP, XX, XU><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec, x, r, red, \
-                                                 cg, nr, rho_rhs)
-  if (p == Prec::F64) { if (xupd) P4(Prec::F64, Prec::F64, true); else P4(Prec::F64, Prec::F64, false); }
-  else if (p == Prec::F32) { if (xupd) P4(Prec::F32, Prec::F32, true); else P4(Prec::F32, Prec::F32, false); }
-  else { if (xupd) P4(Prec::F16, Prec::F32, true); else P4(Prec::F16, Prec::F32, false); }
+#define P4(PP, XX, XU, K)                                                                                   \
+  k_cg_pass4<PP, XX, XU, K><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec, x, r, \
+                                                    red, cg, nr, rho_rhs, op.kappa, kappa_rhs)
+#define P4K(PP, XX, XU) if (g.clover_t) P4(PP, XX, XU, true); else P4(PP, XX, XU, false);
+  if (p == Prec::F64) { if (xupd) { P4K(Prec::F64, Prec::F64, true) } else { P4K(Prec::F64, Prec::F64, false) } }
+  else if (p == Prec::F32) { if (xupd) { P4K(Prec::F32, Prec::F32, true) } else { P4K(Prec::F32, Prec::F32, false) } }
+  else { if (xupd) { P4K(Prec::F16, Prec::F32, true) } else { P4K(Prec::F16, Prec::F32, false) } }
+#undef P4K
 #undef P4
 }
 

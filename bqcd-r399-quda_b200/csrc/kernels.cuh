@@ -75,19 +75,25 @@ void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStrea
 // first half of mtil / mtil_dag: out_o = [(1 -+ i h g5)] Ainv_oo D_oe in_e
 // (nr > 1: nr right-hand sides in one launch, fields at SpinorPtr::rsb strides,
 //  cg / norm_out arrays of nr entries; retired RHS return at once)
+// (g.clover_t: the clover fields hold T and each pass forms A(kappa) and
+//  A(kappa)^-1 per site, at op.kappa or at kappa_rhs[k] for right-hand side k;
+//  kappa_rhs also sets each right-hand side's hopping coefficient)
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
-                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr = 1);
+                       CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr = 1,
+                       const double* kappa_rhs = nullptr);
 // second half: out_e = A_ee in_e + b D_eo t_o (+ h term for Wilson) + rho in_e;
 // optional |out|^2 reduction into *norm_out (device), and CG alpha update
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s, int nr = 1, const double* rho_rhs = nullptr);
+                       CgScalars* cg, cudaStream_t s, int nr = 1, const double* rho_rhs = nullptr,
+                       const double* kappa_rhs = nullptr);
 // CG-fused second half of mtil_dag: Ap = A_ee q + b D_eo t_o + rho q computed in
 // registers; x += alpha p, r -= alpha Ap, rtr = |r|^2.  Precision P for the
 // stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr = 1, bool xupd = true, const double* rho_rhs = nullptr);
+                     cudaStream_t s, int nr = 1, bool xupd = true, const double* rho_rhs = nullptr,
+                     const double* kappa_rhs = nullptr);
 // (rho_rhs: device array of one shift rho per right-hand side, replacing
 //  op.rho, in the second passes; null: op.rho for all)
 // register-blocked batched passes (dslash_multi.cu): one thread serves one
@@ -178,6 +184,10 @@ void launch_clover_d(const Geom& g, double* p, const double2* gauge, const doubl
 int clover_init_chunk(const Geom& g);
 void launch_clover_init(const Geom& g, const double2* gauge, double csw_kappa, double2* a[2], double2* ainv[2],
                         double2* b[2], double2* tmp, cudaStream_t s);
+// T = (-c_sw / 8)(p +- q) of each chiral block, packed like A, for the
+// parities whose pointer is given: the kappa-independent part of the clover
+// term, A(kappa) = 1 + kappa T (clover_init.F90:46-77, clover_init3)
+void launch_clover_t(const Geom& g, const double2* gauge, double csw, double2* t[2], double2* tmp, cudaStream_t s);
 // 2 sum log det over the halved 1/D of B (clover_action.F90)
 void launch_clover_action(const Geom& g, const double2* b, RedScratch red, double* out, cudaStream_t s);
 

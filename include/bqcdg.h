@@ -141,6 +141,17 @@ int bqcdg_clover_init(bqcdg_ctx *ctx, double csw_kappa);
  * A third of the memory of bqcdg_clover_init, for lattices where all six do
  * not fit; entry points that need the others then return BQCDG_ENOCLOVER. */
 int bqcdg_clover_init_solver(bqcdg_ctx *ctx, double csw_kappa);
+/* the clover term for any hopping parameter: clover_init.F90:46-77 builds
+ * each chiral block as 1 + (-c_sw kappa / 8)(p +- q) from field strengths
+ * that do not depend on kappa.  This stores T = (-c_sw / 8)(p +- q) of the
+ * even and the odd sites from the loaded links; the operators then form
+ * A(kappa) = 1 + kappa T and the LDL^+ solve of A(kappa) per site, at the
+ * kappa of their parameters (p->csw_kappa only has to be nonzero).  It is
+ * what bqcdg_solve_batch_kappa needs for systems with different kappa.
+ * Entry points that read BQCD's clover blocks themselves (clover_mult_*,
+ * get_clover, the forces) return BQCDG_EUNSUPPORTED until a clover_init or
+ * load_clover replaces T. */
+int bqcdg_clover_init_t(bqcdg_ctx *ctx, double csw);
 /* clover_action(b(1,1,ODD)) (clover/clover_action.F90:29) */
 int bqcdg_clover_action(bqcdg_ctx *ctx, int eo, double *action);
 
@@ -236,6 +247,16 @@ int bqcdg_solve_batch(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, co
 int bqcdg_solve_batch_shifted(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
                               const double *rho, const double *tol, const bqcdg_solver_opts *o, int block,
                               bqcdg_solve_info *infos);
+/* bqcdg_solve_batch_shifted with a hopping parameter per right-hand side:
+ * system k is (W_k^+W_k) x_k = b_k with W_k = M~(kappa[k]) + rho[k] (rho NULL:
+ * p->rho for all), its own clover term from bqcdg_clover_init_t when
+ * p->csw_kappa != 0 (BQCDG_ENOCLOVER otherwise) and its own hopping
+ * coefficient -kappa[k]^2 / (1 + h^2) (m_tilde.F90:67).  These are the
+ * systems of a spectrum of quark masses on one gauge field; their FP64
+ * reliable updates and true residuals use their own operators. */
+int bqcdg_solve_batch_kappa(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
+                            const double *kappa, const double *rho, const double *tol, const bqcdg_solver_opts *o,
+                            int block, bqcdg_solve_info *infos);
 /* out = (W^+W) in with both resident, repeated n times; *ms = average device
  * time of one application (CUDA events on the context stream) */
 int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);
