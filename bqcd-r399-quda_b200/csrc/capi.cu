@@ -1637,7 +1637,7 @@ int bqcdg_time_pass_batch(bqcdg_ctx* c, int nrhs, const int* hin, const bqcdg_pa
   if (st) return st;
   if (!hin || nrhs <= 0 || nrhs > kMaxRhs || n <= 0) return BQCDG_EINVAL;
   if (rhs_per_thread != 0 && rhs_per_thread != 1 && rhs_per_thread != 2 && rhs_per_thread != 4) return BQCDG_EINVAL;
-  if (rhs_per_thread > 1 && p->h != 0.0) return BQCDG_EUNSUPPORTED;
+  if (rhs_per_thread > 1 && (p->h != 0.0 || c->g.clover_t)) return BQCDG_EUNSUPPORTED;
   for (int k = 0; k < nrhs; k++)
     if (!field(c, hin[k])) return BQCDG_EINVAL;
   Prec pr = prec_of(precision);
