@@ -99,6 +99,7 @@ def _lib_handle():
         L.bqcdg_clover_init.argtypes = [vp, C.c_double]
         L.bqcdg_clover_init_solver.argtypes = [vp, C.c_double]
         L.bqcdg_clover_init_t.argtypes = [vp, C.c_double]
+        L.bqcdg_solve_block.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), P(SolverOpts), P(SolveInfo)]
         L.bqcdg_solve_batch_kappa.argtypes = [vp, i, P(C.c_int), P(C.c_int), P(Params), dp, dp, dp,
                                               P(SolverOpts), i, P(SolveInfo)]
         L.bqcdg_release_scratch.argtypes = [vp, i]
@@ -602,6 +603,22 @@ class Lattice:
                                              r.ctypes.data, tols.ctypes.data, C.byref(o), block, infos)
         if st not in (OK, ENOCONV):
             _check(st, "solve_batch_shifted")
+        return list(infos)
+
+    def solve_block(self, hxs, hbs, para, tol=1e-10, relative=True, maxiter=100000, delta=0.1, rho=None):
+        """Block CG over the resident systems (W^+W) x_k = b_k (up to 16)
+        sharing one Krylov space: FP32 blocks, FP64 restarts.  Returns the
+        infos (niter = block iterations until the system left)."""
+        n = len(hxs)
+        if len(hbs) != n:
+            raise ValueError("solve_block: one b per x")
+        o = SolverOpts(PREC_SINGLE, maxiter, int(relative), tol, delta, 1, 0, 1)
+        infos = (SolveInfo * n)()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        st = lib().bqcdg_solve_block(self.h, n, (C.c_int * n)(*hxs), (C.c_int * n)(*hbs), C.byref(prm), C.byref(o),
+                                     infos)
+        if st not in (OK, ENOCONV):
+            _check(st, "solve_block")
         return list(infos)
 
     def clover_init_t(self, csw):

@@ -768,6 +768,15 @@ int bqcdg_release_scratch(bqcdg_ctx* c, int what) {
       pool->clear();
     }
     auto& B = c->batch;
+    auto& K = c->blk;
+    for (SpinorPtr* sp : {&K.P, &K.Q, &K.Z, &K.M, &K.Xs, &K.T, &K.Qe}) {
+      c->release(sp->v);
+      *sp = SpinorPtr{};
+    }
+    c->release(K.partial);
+    c->release(K.gram);
+    c->release(K.mats);
+    K = bqcdg_ctx::BlockCg{};
     for (SpinorPtr* sp : {&B.p, &B.t, &B.q, &B.rs, &B.xs}) {
       c->release(sp->v);
       c->release(sp->norm);

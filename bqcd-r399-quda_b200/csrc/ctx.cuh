@@ -81,6 +81,16 @@ struct bqcdg_ctx {
     Prec prec = Prec::F64;
     SpinorPtr p, t, q, rs, xs;
   } batch;
+  // FP32 blocks of the block CG (capi_block.cu): search, residual basis,
+  // A times search, scratch, solution increments, and the two intermediate
+  // fields of the operator, cap fields each; Gram sums and s x s matrices
+  struct BlockCg {
+    int cap = 0;
+    SpinorPtr P, Q, Z, M, Xs, T, Qe;
+    double2* partial = nullptr;
+    double2* gram = nullptr;
+    float2* mats = nullptr;
+  } blk;
   int tuned_block[3] = {0, 0, 0};  // chosen RHS per launch, by precision
   int tuned_nbt[3][17] = {};       // chosen RHS per stencil thread, by precision and RHS per launch
 

@@ -115,6 +115,18 @@ void launch_cg_pass4_n(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, cons
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,
                        int nr = 1, SpinorPtr x = SpinorPtr{}, int expect = -1);
 
+// ---- block solver (blockcg.cu) ----
+// out[i * s + j] = <a_i, b_j> (FP64) for two blocks of s <= 16 FP32 fields
+// (batched layout); partial: block_gram_scratch_pairs() complex doubles
+int block_gram_scratch_pairs();
+void launch_block_gram(const Geom& g, int s, SpinorPtr a, SpinorPtr b, double2* partial, double2* out,
+                       cudaStream_t st);
+// out_j = sum_k in1_k m1[k * s + j] (+ sum_k in2_k m2[k * s + j] when in2.v):
+// right multiplication of FP32 blocks by s x s complex matrices; out may be
+// in1 or in2
+void launch_block_combine(const Geom& g, int s, SpinorPtr out, SpinorPtr in1, const float2* m1, SpinorPtr in2,
+                          const float2* m2, cudaStream_t st);
+
 // ---- configuration files (confio.cu) ----
 // time slice t of the resident FP64 links in the order and byte order of
 // BQCD's slice files (24 big-endian complex per site, 384 bytes), and back

@@ -257,6 +257,19 @@ int bqcdg_solve_batch_shifted(bqcdg_ctx *ctx, int nrhs, const int *hx, const int
 int bqcdg_solve_batch_kappa(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
                             const double *kappa, const double *rho, const double *tol, const bqcdg_solver_opts *o,
                             int block, bqcdg_solve_info *infos);
+/* block CG over nrhs <= 16 resident systems (W^+W) x_k = b_k that share W
+ * (W = M~ + p->rho), e.g. the point sources of a propagator: one Krylov
+ * space for all of them (O'Leary's block CG in the residual-QR form of
+ * Dubrulle, 2001), searched along nrhs directions per iteration, so the
+ * systems need fewer iterations than alone.  FP32 blocks
+ * (o->precision = BQCDG_PREC_SINGLE), restarted from FP64 residuals when the
+ * largest residual has dropped by o->delta; a system that reaches its
+ * tolerance at a restart leaves the block.  infos[k].niter: block
+ * iterations until system k left; reliable_updates: restarts; true_rtr: its
+ * last FP64 |b - A x|^2.  The reference solves its systems one at a time
+ * (cg.F90:51). */
+int bqcdg_solve_block(bqcdg_ctx *ctx, int nrhs, const int *hx, const int *hb, const bqcdg_params *p,
+                      const bqcdg_solver_opts *o, bqcdg_solve_info *infos);
 /* out = (W^+W) in with both resident, repeated n times; *ms = average device
  * time of one application (CUDA events on the context stream) */
 int bqcdg_mdagm_dev(bqcdg_ctx *ctx, int hout, int hin, const bqcdg_params *p, int precision, int n, double *ms);
