@@ -590,7 +590,9 @@ def run_batch(args):
     batch_s = allmax(pg, time.perf_counter() - t0, local)
     dx = max(float(np.linalg.norm(lat.field_get(hxs[k]) - seq[n]["x"]) / np.linalg.norm(seq[n]["x"]))
              for n, k in (("point", 0), ("gauss", 12)))
-    # block CG arm: one Krylov space for the 16 systems
+    # block CG arm: one Krylov space for the 16 systems (its seven FP32 blocks
+    # need the memory of the batched solver's buffers, released first)
+    lat.release_scratch(solver=True)
     reset()
     barrier(pg, local)
     t0 = time.perf_counter()
