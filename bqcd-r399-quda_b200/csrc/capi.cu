@@ -235,14 +235,16 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     nl += 5 * batch;
     const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
-      // pass 1 (timed), pass 2 (+|M~p|^2 -> alpha), pass 3, pass 4 (+x,r update, |r|^2), p update
+      // pass 1 (timed), pass 2 (+|M~p|^2 partials), pass 3 (+ their sum -> alpha), pass 4 (+x,r update,
+      // |r|^2), p update
       kt.begin();
       launch_mtil_pass1(sloppy, gs, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
       kt.end();
       launch_mtil_pass2(sloppy, gs, false, q, t, p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
-                        c->dcg, c->stream);
+                        c->dcg, c->stream, 1, nullptr, nullptr, true);
       kt.begin();
-      launch_mtil_pass1(sloppy, gs, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
+      launch_mtil_pass1(sloppy, gs, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream, 1,
+                        nullptr, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
       kt.end();
       launch_cg_pass4(sloppy, gs, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
                       c->stream, 1, false);
@@ -491,9 +493,9 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
         launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
                           c->stream, nb, dkap);
         launch_mtil_pass2(sloppy, g, false, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red,
-                          nullptr, c->dcg, c->stream, nb, drho, dkap);
+                          nullptr, c->dcg, c->stream, nb, drho, dkap, true);
         launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
-                          c->stream, nb, dkap);
+                          c->stream, nb, dkap, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
         launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
                         c->dcg, c->stream, nb, true, drho, dkap);
       }

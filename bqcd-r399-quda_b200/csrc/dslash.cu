@@ -165,10 +165,21 @@ void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStrea
 template <Prec P, bool DAG, bool KT>
 __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge,
                                                   CloverPtr ainv, int has_clover, double hval, const CgScalars* cg,
-                                                  int nr, double kappa, const double* kappa_rhs) {
+                                                  int nr, double kappa, const double* kappa_rhs, AlphaFin fin) {
   using R = typename SpinorView<P>::R;
   const Tile tl = tile(nr);
   if (cg && cg[tl.rhs].done) return;  // retired right-hand side
+  if (fin.partial && tl.sb == 0) {
+    // alpha of the k_pass2 before (launched with defer_alpha); the first
+    // CTAs of a launch run this while the others start on their sites
+    double tot[1];
+    final_sum<1>(fin.partial + (size_t)tl.rhs * kRedVals * fin.stride, fin.stride, tl.nsb, tot);
+    if (threadIdx.x == 0) {
+      CgScalars* c = fin.cg + tl.rhs;
+      c->paap = tot[0];
+      c->alpha = c->rtr / tot[0];
+    }
+  }
   const int i = tl.i;
   if (i >= g.volh) return;
   auto in = sview<P>(rhs_of(inp, tl.rhs), g.stride);
@@ -192,12 +203,12 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks) k_pass1(Geom g, Sp
 
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
                        CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr,
-                       const double* kappa_rhs) {
+                       const double* kappa_rhs, AlphaFin fin) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double hv = dag ? op.h : -op.h;
 #define P1(PP, D, K) \
-  k_pass1<PP, D, K><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr, op.kappa, kappa_rhs)
+  k_pass1<PP, D, K><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr, op.kappa, kappa_rhs, fin)
 #define P1K(PP, D) if (g.clover_t) P1(PP, D, true); else P1(PP, D, false);
   if (p == Prec::F64) { if (dag) { P1K(Prec::F64, true) } else { P1K(Prec::F64, false) } }
   else if (p == Prec::F32) { if (dag) { P1K(Prec::F32, true) } else { P1K(Prec::F32, false) } }
@@ -258,7 +269,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
                                                   const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                                                   double hval, double rho, RedScratch red, double* norm_out,
                                                   CgScalars* cg, int nr, const double* rho_rhs, double kappa,
-                                                  const double* kappa_rhs) {
+                                                  const double* kappa_rhs, bool defer_alpha) {
   using R = typename SpinorView<P>::R;
   const Tile tl = tile(nr);
   if (cg && cg[tl.rhs].done) return;  // retired right-hand side
@@ -287,7 +298,10 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
   if (REDUCE) {
     double* part = red.partial + (size_t)tl.rhs * kRedVals * red.maxblocks;
     block_reduce_store<1>(acc, part, red.maxblocks, tl.sb);
-    if (last_block(red.counter + tl.rhs, tl.nsb)) {
+    // defer_alpha: the partials stay for the next k_pass1 (AlphaFin).  The
+    // arrival counter of the last-block sum costs a k_pass2<int16> at 32^3x64
+    // 8 % of its time (137 against 127 us), its partial stores alone nothing.
+    if (!defer_alpha && last_block(red.counter + tl.rhs, tl.nsb)) {
       double tot[1];
       final_sum<1>(part, red.maxblocks, tl.nsb, tot);
       if (threadIdx.x == 0) {
@@ -305,15 +319,17 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_pass2(Geom g, S
 
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
-                       CgScalars* cg, cudaStream_t s, int nr, const double* rho_rhs, const double* kappa_rhs) {
+                       CgScalars* cg, cudaStream_t s, int nr, const double* rho_rhs, const double* kappa_rhs,
+                       bool defer_alpha) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = dag ? -op.h : op.h;
   bool reduce = norm_out != nullptr || cg != nullptr;
+  defer_alpha = defer_alpha && cg && !norm_out;  // only alpha can wait for the next pass
 #define P2(PP, D, RR, K)                                                                                        \
   k_pass2<PP, D, RR, K><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, hv, op.rho, red, \
-                                                norm_out, cg, nr, rho_rhs, op.kappa, kappa_rhs)
+                                                norm_out, cg, nr, rho_rhs, op.kappa, kappa_rhs, defer_alpha)
 #define P2R(PP, D)                                         \
   if (g.clover_t) {                                        \
     if (reduce) P2(PP, D, true, true); else P2(PP, D, false, true);   \

@@ -78,15 +78,26 @@ void launch_clover_mult_b(const Geom& g, double2* x, const double2* b, cudaStrea
 // (g.clover_t: the clover fields hold T and each pass forms A(kappa) and
 //  A(kappa)^-1 per site, at op.kappa or at kappa_rhs[k] for right-hand side k;
 //  kappa_rhs also sets each right-hand side's hopping coefficient)
+// The |M~ p|^2 block partials that a k_pass2 launched with defer_alpha left
+// in red.partial (slot 0 of each RHS).  The k_pass1 launch after it, given
+// this, sums them in its first site block of each RHS, before its own sites,
+// and sets that RHS's paap and alpha = rtr / paap: the same fixed-order sum
+// (final_sum) that k_pass2's last block would run, so alpha is bit for bit
+// the same, but no k_pass2 block waits for an arrival counter.
+struct AlphaFin {
+  const double* partial = nullptr;
+  int stride = 0;  // RedScratch::maxblocks
+  CgScalars* cg = nullptr;
+};
 void launch_mtil_pass1(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
                        CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr = 1,
-                       const double* kappa_rhs = nullptr);
+                       const double* kappa_rhs = nullptr, AlphaFin fin = AlphaFin{});
 // second half: out_e = A_ee in_e + b D_eo t_o (+ h term for Wilson) + rho in_e;
 // optional |out|^2 reduction into *norm_out (device), and CG alpha update
 void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e,
                        const void* gauge, CloverPtr a_ee, const OpParams& op, RedScratch red, double* norm_out,
                        CgScalars* cg, cudaStream_t s, int nr = 1, const double* rho_rhs = nullptr,
-                       const double* kappa_rhs = nullptr);
+                       const double* kappa_rhs = nullptr, bool defer_alpha = false);
 // CG-fused second half of mtil_dag: Ap = A_ee q + b D_eo t_o + rho q computed in
 // registers; x += alpha p, r -= alpha Ap, rtr = |r|^2.  Precision P for the
 // stencil fields, x/r in XP (F64 for the FP64 solver, F32 for the sloppy one)

@@ -98,3 +98,31 @@ def test_noalloc_matches_context_entry_point_twice(oracle, bq, fn, rho):
             ref = lat.w_dagger_w(psi, para) if rho else lat.mtdagmt(psi, para)
             assert np.linalg.norm(got - ref) <= TOL64 * np.linalg.norm(ref), call
 
+
+def test_noalloc_without_clover_on_a_caller_stream(oracle, bq, fn):
+    """csw = 0 (a_even and ainv_odd NULL, the Wilson operator with h) and the
+    work enqueued on a stream of the caller's rather than the default one."""
+    import torch
+    L, bc = (4, 6, 8, 4), (1, 1, 1, -1)
+    g = oracle.Geom(L, bc)
+    oracle.ranset(32)
+    u = g.hot()
+    para = bq.HmcPara(kappa=0.125, csw=0.0, h=0.05)
+    volh = g.volh
+    d_u = dev(gauge_layout(u, volh), torch)
+    psi = g.gauss_spinor(0)
+    d_in = dev(spinor_layout(psi, volh), torch)
+    d_out = torch.full_like(d_in, float("nan"))
+    torch.cuda.synchronize()
+    Li, bci = (C.c_int * 4)(*L), (C.c_int * 4)(*bc)
+    prm = para.params()
+    s = torch.cuda.Stream()
+    st = fn(Li, bci, d_u.data_ptr(), None, None, C.byref(prm), d_in.data_ptr(), d_out.data_ptr(),
+            C.c_void_p(s.cuda_stream))
+    assert st == bq.OK
+    s.synchronize()
+    got = spinor_from_layout(d_out.cpu().numpy(), volh)
+    with bq.Lattice(L, bc) as lat:
+        lat.load_gauge(u, flipped=False)
+        ref = lat.mtdagmt(psi, para)
+    assert np.linalg.norm(got - ref) <= TOL64 * np.linalg.norm(ref)
