@@ -232,7 +232,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
   int batch = 4;
   const Geom& gs = geom_of(c, sloppy);  // stencil geometry (12-real FP64 links when SU(3))
   while (!h.done) {
-    nl += 5 * batch;
+    nl += 6 * batch;
     const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
       // pass 1 (timed), pass 2 (+|M~p|^2 partials), pass 3 (+ their sum -> alpha), pass 4 (+x,r update,
@@ -247,7 +247,8 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
                         nullptr, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
       kt.end();
       launch_cg_pass4(sloppy, gs, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
-                      c->stream, 1, false);
+                      c->stream, 1, false, nullptr, nullptr, true);
+      launch_cg_step(c->red, c->dcg, 1, nblocks(gs.volh), c->stream);
       launch_cg_pupdate(sloppy, g, p, rs, c->dcg, c->stream, 1, xs, iter0 + k + 1);
     }
     CKL();
@@ -497,11 +498,12 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
         launch_mtil_pass1(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
                           c->stream, nb, dkap, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
         launch_cg_pass4(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
-                        c->dcg, c->stream, nb, true, drho, dkap);
+                        c->dcg, c->stream, nb, true, drho, dkap, true);
+        launch_cg_step(c->red, c->dcg, nb, nblocks(g.volh), c->stream);
       }
       launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
     }
-    launches += 5 * batch;
+    launches += (nbt > 1 ? 5 : 6) * batch;
     CKL();
     CK(cudaMemcpyAsync(c->hcg, c->dcg, sizeof(CgScalars) * nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
                                                      CloverPtr aee, int has_clover, double bcoef, double hval,
                                                      double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp,
                                                      RedScratch red, CgScalars* cgs, int nr, const double* rho_rhs,
-                                                     double kappa, const double* kappa_rhs) {
+                                                     double kappa, const double* kappa_rhs, bool defer_step) {
   using R = typename SpinorView<P>::R;
   using RX = typename SpinorView<XP>::R;
   const Tile tl = tile(nr);
@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
   }
   double* part = red.partial + (size_t)tl.rhs * kRedVals * red.maxblocks;
   block_reduce_store<1>(acc, part, red.maxblocks, tl.sb);
-  if (last_block(red.counter + tl.rhs, tl.nsb)) {
+  if (!defer_step && last_block(red.counter + tl.rhs, tl.nsb)) {
     double tot[1];
     final_sum<1>(part, red.maxblocks, tl.nsb, tot);
     if (threadIdx.x == 0) {
@@ -424,16 +424,32 @@ __global__ void __launch_bounds__(kBlock, Occ<P>::min_blocks2) k_cg_pass4(Geom g
   }
 }
 
+// the deferred step of k_cg_pass4 (defer_step): CTA r sums RHS r's partials
+// with all its threads in flight at once and steps its scalars
+constexpr int kStepBlock = 1024;
+__global__ void __launch_bounds__(kStepBlock) k_cg_step(RedScratch red, CgScalars* cgs, int nsb) {
+  CgScalars* cg = cgs + blockIdx.x;
+  if (cg->done) return;  // k_cg_pass4 did not run for this right-hand side
+  double tot[1];
+  final_sum<1>(red.partial + (size_t)blockIdx.x * kRedVals * red.maxblocks, red.maxblocks, nsb, tot);
+  if (threadIdx.x == 0) cg_scalar_step(cg, tot[0]);
+}
+
+void launch_cg_step(RedScratch red, CgScalars* cg, int nr, int nsb, cudaStream_t s) {
+  k_cg_step<<<nr, kStepBlock, 0, s>>>(red, cg, nsb);
+}
+
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                     cudaStream_t s, int nr, bool xupd, const double* rho_rhs, const double* kappa_rhs) {
+                     cudaStream_t s, int nr, bool xupd, const double* rho_rhs, const double* kappa_rhs,
+                     bool defer_step) {
   dim3 grid(nblocks(g.volh) * nr);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   double hv = -op.h;  // mtil_dag
 #define P4(PP, XX, XU, K)                                                                                   \
   k_cg_pass4<PP, XX, XU, K><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, hv, op.rho, pvec, x, r, \
-                                                    red, cg, nr, rho_rhs, op.kappa, kappa_rhs)
+                                                    red, cg, nr, rho_rhs, op.kappa, kappa_rhs, defer_step)
 #define P4K(PP, XX, XU) if (g.clover_t) P4(PP, XX, XU, true); else P4(PP, XX, XU, false);
   if (p == Prec::F64) { if (xupd) { P4K(Prec::F64, Prec::F64, true) } else { P4K(Prec::F64, Prec::F64, false) } }
   else if (p == Prec::F32) { if (xupd) { P4K(Prec::F32, Prec::F32, true) } else { P4K(Prec::F32, Prec::F32, false) } }

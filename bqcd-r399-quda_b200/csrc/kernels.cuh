@@ -104,7 +104,14 @@ void launch_mtil_pass2(Prec p, const Geom& g, bool dag, SpinorPtr out_e, SpinorP
 void launch_cg_pass4(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                      const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
                      cudaStream_t s, int nr = 1, bool xupd = true, const double* rho_rhs = nullptr,
-                     const double* kappa_rhs = nullptr);
+                     const double* kappa_rhs = nullptr, bool defer_step = false);
+// With defer_step, k_cg_pass4 leaves its |r|^2 block partials in red.partial
+// and launch_cg_step, queued after it, sums them (one CTA per right-hand
+// side, the fixed-order final_sum) and takes the CG scalar step
+// (cg_scalar_step: beta, the stop tests), which the last k_cg_pass4 block
+// would otherwise take after an arrival counter.  nsb: site blocks per RHS
+// of that k_cg_pass4 launch.
+void launch_cg_step(RedScratch red, CgScalars* cg, int nr, int nsb, cudaStream_t s);
 // (rho_rhs: device array of one shift rho per right-hand side, replacing
 //  op.rho, in the second passes; null: op.rho for all)
 // register-blocked batched passes (dslash_multi.cu): one thread serves one
