@@ -485,11 +485,12 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
         launch_mtil_pass1_n(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
                             c->stream, nb, nbt);
         launch_mtil_pass2_n(sloppy, g, B.q, B.t, B.p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, c->dcg,
-                            c->stream, nb, drho, nbt);
+                            c->stream, nb, drho, nbt, true);
         launch_mtil_pass1_n(sloppy, g, true, B.t, B.q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
-                            c->stream, nb, nbt);
+                            c->stream, nb, nbt, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
         launch_cg_pass4_n(sloppy, g, B.t, B.q, gauge_of(c, sloppy), aee_of(c, sloppy), op, B.p, B.xs, B.rs, c->red,
-                          c->dcg, c->stream, nb, drho, nbt);
+                          c->dcg, c->stream, nb, drho, nbt, true);
+        launch_cg_step(c->red, c->dcg, nb, nblocks(g.volh), c->stream);
       } else {
         launch_mtil_pass1(sloppy, g, false, B.t, B.p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg,
                           c->stream, nb, dkap);
@@ -503,7 +504,7 @@ int cg_batch(bqcdg_ctx* c, double2** x, double2** b, int nb, const OpParams& op,
       }
       launch_cg_pupdate(sloppy, g, B.p, B.rs, c->dcg, c->stream, nb);
     }
-    launches += (nbt > 1 ? 5 : 6) * batch;
+    launches += 6 * batch;
     CKL();
     CK(cudaMemcpyAsync(c->hcg, c->dcg, sizeof(CgScalars) * nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -193,12 +193,26 @@ struct OccN {
 template <Prec P, bool DAG, int NB>
 __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
     k_pass1_n(Geom g, SpinorPtr outp, SpinorPtr inp, const void* gauge, CloverPtr ainv, int has_clover, double hval,
-              const CgScalars* cg, int nr, int ng) {
+              const CgScalars* cg, int nr, int ng, AlphaFin fin) {
   using R = typename SpinorView<P>::R;
   const GTile tl = gtile(ng);
   const int rhs0 = tl.grp * NB;
   bool act[NB];
   if (!group_live<NB>(cg, rhs0, nr, act)) return;
+  if (fin.partial && tl.sb == 0) {
+    // alpha of the k_pass2_n before (defer_alpha), as in k_pass1
+    double tot[NB];
+    final_sum<NB>(fin.partial + (size_t)rhs0 * kRedVals * fin.stride, kRedVals * fin.stride, tl.nsb, tot);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int r = 0; r < NB; r++) {
+        if (!act[r]) continue;
+        CgScalars* c = fin.cg + rhs0 + r;
+        c->paap = tot[r];
+        c->alpha = c->rtr / tot[r];
+      }
+    }
+  }
   const int i = tl.i;
   if (i >= g.volh) return;
   SpinorView<P> in[NB];
@@ -225,12 +239,13 @@ __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
 
 void launch_mtil_pass1_n(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
                          CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr,
-                         int nbt) {
+                         int nbt, AlphaFin fin) {
   const int ng = (nr + nbt - 1) / nbt;
   dim3 grid(nblocks(g.volh) * ng);
   int hc = op.csw_kappa != 0.0;
   double hv = dag ? op.h : -op.h;
-#define P1N(PP, D, N) k_pass1_n<PP, D, N><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr, ng)
+#define P1N(PP, D, N) \
+  k_pass1_n<PP, D, N><<<grid, kBlock, 0, s>>>(g, out_o, in_e, gauge, ainv_oo, hc, hv, cg, nr, ng, fin)
 #define P1NB(PP, N) \
   if (dag) P1N(PP, true, N); else P1N(PP, false, N)
   if (p == Prec::F32) { if (nbt == 2) { P1NB(Prec::F32, 2); } else { P1NB(Prec::F32, 4); } }
@@ -302,7 +317,8 @@ __device__ __forceinline__ void group_rho(double rho, const double* rho_rhs, int
 template <Prec P, int NB>
 __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
     k_pass2_n(Geom g, SpinorPtr outp, SpinorPtr tp, SpinorPtr xp, const void* gauge, CloverPtr aee, int has_clover,
-              double bcoef, double rho, RedScratch red, CgScalars* cg, int nr, int ng, const double* rho_rhs) {
+              double bcoef, double rho, RedScratch red, CgScalars* cg, int nr, int ng, const double* rho_rhs,
+              bool defer_alpha) {
   using R = typename SpinorView<P>::R;
   const GTile tl = gtile(ng);
   const int rhs0 = tl.grp * NB;
@@ -336,7 +352,7 @@ __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
   // value r of the group goes to the partial slot of RHS rhs0 + r
   double* part = red.partial + (size_t)rhs0 * kRedVals * red.maxblocks;
   block_reduce_store<NB>(acc, part, kRedVals * red.maxblocks, tl.sb);
-  if (last_block(red.counter + rhs0, tl.nsb)) {
+  if (!defer_alpha && last_block(red.counter + rhs0, tl.nsb)) {
     double tot[NB];
     final_sum<NB>(part, kRedVals * red.maxblocks, tl.nsb, tot);
     if (threadIdx.x == 0) {
@@ -354,14 +370,14 @@ __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
 
 void launch_mtil_pass2_n(Prec p, const Geom& g, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e, const void* gauge,
                          CloverPtr a_ee, const OpParams& op, RedScratch red, CgScalars* cg, cudaStream_t s, int nr,
-                         const double* rho_rhs, int nbt) {
+                         const double* rho_rhs, int nbt, bool defer_alpha) {
   const int ng = (nr + nbt - 1) / nbt;
   dim3 grid(nblocks(g.volh) * ng);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa;  // h = 0
 #define P2N(PP, N)                                                                                          \
   k_pass2_n<PP, N><<<grid, kBlock, 0, s>>>(g, out_e, t_o, in_e, gauge, a_ee, hc, bcoef, op.rho, red, cg, nr, ng, \
-                                           rho_rhs)
+                                           rho_rhs, defer_alpha)
   if (p == Prec::F32) { if (nbt == 2) P2N(Prec::F32, 2); else P2N(Prec::F32, 4); }
   else { if (nbt == 2) P2N(Prec::F16, 2); else P2N(Prec::F16, 4); }
 #undef P2N
@@ -374,7 +390,7 @@ template <Prec P, int NB>
 __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
     k_cg_pass4_n(Geom g, SpinorPtr tp, SpinorPtr qp, const void* gauge, CloverPtr aee, int has_clover, double bcoef,
                  double rho, SpinorPtr pp, SpinorPtr xp, SpinorPtr rp, RedScratch red, CgScalars* cgs, int nr, int ng,
-                 const double* rho_rhs) {
+                 const double* rho_rhs, bool defer_step) {
   using R = typename SpinorView<P>::R;
   const GTile tl = gtile(ng);
   const int rhs0 = tl.grp * NB;
@@ -433,7 +449,7 @@ __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
   }
   double* part = red.partial + (size_t)rhs0 * kRedVals * red.maxblocks;
   block_reduce_store<NB>(acc, part, kRedVals * red.maxblocks, tl.sb);
-  if (last_block(red.counter + rhs0, tl.nsb)) {
+  if (!defer_step && last_block(red.counter + rhs0, tl.nsb)) {
     double tot[NB];
     final_sum<NB>(part, kRedVals * red.maxblocks, tl.nsb, tot);
     if (threadIdx.x == 0) {
@@ -449,14 +465,14 @@ __global__ void __launch_bounds__(kBlock, OccN<NB>::min_blocks)
 
 void launch_cg_pass4_n(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                        const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                       cudaStream_t s, int nr, const double* rho_rhs, int nbt) {
+                       cudaStream_t s, int nr, const double* rho_rhs, int nbt, bool defer_step) {
   const int ng = (nr + nbt - 1) / nbt;
   dim3 grid(nblocks(g.volh) * ng);
   int hc = op.csw_kappa != 0.0;
   double bcoef = -op.kappa * op.kappa;  // h = 0
 #define P4N(PP, N)                                                                                              \
   k_cg_pass4_n<PP, N><<<grid, kBlock, 0, s>>>(g, t_o, q_e, gauge, a_ee, hc, bcoef, op.rho, pvec, x, r, red, cg, nr, \
-                                              ng, rho_rhs)
+                                              ng, rho_rhs, defer_step)
   if (p == Prec::F32) { if (nbt == 2) P4N(Prec::F32, 2); else P4N(Prec::F32, 4); }
   else { if (nbt == 2) P4N(Prec::F16, 2); else P4N(Prec::F16, 4); }
 #undef P4N

@@ -121,13 +121,13 @@ void launch_cg_step(RedScratch red, CgScalars* cg, int nr, int nsb, cudaStream_t
 // pass 4 updates x (cg required for both).
 void launch_mtil_pass1_n(Prec p, const Geom& g, bool dag, SpinorPtr out_o, SpinorPtr in_e, const void* gauge,
                          CloverPtr ainv_oo, const OpParams& op, const CgScalars* cg, cudaStream_t s, int nr,
-                         int nbt);
+                         int nbt, AlphaFin fin = AlphaFin{});
 void launch_mtil_pass2_n(Prec p, const Geom& g, SpinorPtr out_e, SpinorPtr t_o, SpinorPtr in_e, const void* gauge,
                          CloverPtr a_ee, const OpParams& op, RedScratch red, CgScalars* cg, cudaStream_t s, int nr,
-                         const double* rho_rhs, int nbt);
+                         const double* rho_rhs, int nbt, bool defer_alpha = false);
 void launch_cg_pass4_n(Prec p, const Geom& g, SpinorPtr t_o, SpinorPtr q_e, const void* gauge, CloverPtr a_ee,
                        const OpParams& op, SpinorPtr pvec, SpinorPtr x, SpinorPtr r, RedScratch red, CgScalars* cg,
-                       cudaStream_t s, int nr, const double* rho_rhs, int nbt);
+                       cudaStream_t s, int nr, const double* rho_rhs, int nbt, bool defer_step = false);
 // p = r + beta p; with x given (xupd = false above, single RHS), also the
 // x += alpha p of iteration `expect` if that iteration ran
 void launch_cg_pupdate(Prec p, const Geom& g, SpinorPtr pvec, SpinorPtr r, CgScalars* cg, cudaStream_t s,
