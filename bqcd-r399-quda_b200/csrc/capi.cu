@@ -235,17 +235,20 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     nl += 6 * batch;
     const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
-      // pass 1 (timed), pass 2 (+|M~p|^2 partials), pass 3 (+ their sum -> alpha), pass 4 (+x,r update,
-      // |r|^2), p update
-      kt.begin();
+      // pass 1, pass 2 (+|M~p|^2 partials), pass 3 (+ their sum -> alpha), pass 4 (+x,r update, |r|^2
+      // partials), the CG step, p update.  With time_kernels, passes 1 and 3 of the first iteration of
+      // each batch are bracketed by events: a sample of every batch, and events between all launches
+      // would lengthen the solve they time.
+      const bool timed = k == 0;
+      if (timed) kt.begin();
       launch_mtil_pass1(sloppy, gs, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
-      kt.end();
+      if (timed) kt.end();
       launch_mtil_pass2(sloppy, gs, false, q, t, p, gauge_of(c, sloppy), aee_of(c, sloppy), op, c->red, nullptr,
                         c->dcg, c->stream, 1, nullptr, nullptr, true);
-      kt.begin();
+      if (timed) kt.begin();
       launch_mtil_pass1(sloppy, gs, true, t, q, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream, 1,
                         nullptr, AlphaFin{c->red.partial, c->red.maxblocks, c->dcg});
-      kt.end();
+      if (timed) kt.end();
       launch_cg_pass4(sloppy, gs, t, q, gauge_of(c, sloppy), aee_of(c, sloppy), op, p, xs, rs, c->red, c->dcg,
                       c->stream, 1, false, nullptr, nullptr, true);
       launch_cg_step(c->red, c->dcg, 1, nblocks(gs.volh), c->stream);
@@ -254,7 +257,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     CKL();
     int st = read_cg(c);
     if (st) return st;
-    kt.collect(2 * (h.iter - iter0));  // two timed passes per iteration run
+    kt.collect(h.iter > iter0 ? 2 : 0);  // the two timed passes ran if the batch's first iteration did
     if (batch < 16) batch *= 2;
     if (h.done == 4) break;
     if (h.done == 0) continue;
@@ -608,8 +611,42 @@ int time_pass1(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int nbt, int re
   return BQCDG_OK;
 }
 
+// device time of one batched M~^+M~ over the batch buffers (the four stencil
+// passes of a CG iteration, the second halves with their reductions but no
+// CG scalars), nbt right-hand sides per thread.  The buffers hold no solve
+// while the tuner runs.
+int time_mdagm_batch(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int nbt, int reps, float* ms) {
+  auto& B = c->batch;
+  const void* U = gauge_of(c, p);
+  auto launch = [&]() {
+    if (nbt > 1) {
+      launch_mtil_pass1_n(p, c->g, false, B.t, B.p, U, ainv_of(c, p), op, nullptr, c->stream, nb, nbt);
+      launch_mtil_pass2_n(p, c->g, B.q, B.t, B.p, U, aee_of(c, p), op, c->red, nullptr, c->stream, nb, nullptr, nbt,
+                          true);
+      launch_mtil_pass1_n(p, c->g, true, B.t, B.q, U, ainv_of(c, p), op, nullptr, c->stream, nb, nbt);
+      launch_mtil_pass2_n(p, c->g, B.p, B.t, B.q, U, aee_of(c, p), op, c->red, nullptr, c->stream, nb, nullptr, nbt,
+                          true);
+    } else {
+      launch_mtil_pass1(p, c->g, false, B.t, B.p, U, ainv_of(c, p), op, nullptr, c->stream, nb);
+      launch_mtil_pass2(p, c->g, false, B.q, B.t, B.p, U, aee_of(c, p), op, c->red, nullptr, nullptr, c->stream, nb);
+      launch_mtil_pass1(p, c->g, true, B.t, B.q, U, ainv_of(c, p), op, nullptr, c->stream, nb);
+      launch_mtil_pass2(p, c->g, true, B.p, B.t, B.q, U, aee_of(c, p), op, c->red, nullptr, nullptr, c->stream, nb);
+    }
+  };
+  launch();
+  CK(cudaEventRecord(c->ev0, c->stream));
+  for (int r = 0; r < reps; r++) launch();
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CKL();
+  CK(cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  cudaEventElapsedTime(&t, c->ev0, c->ev1);
+  *ms = t / reps;
+  return BQCDG_OK;
+}
+
 // right-hand sides per stencil thread for launches of nb at precision p:
-// the fastest first pass of 1, 2 and 4 (timed once, then cached).  The
+// the fastest batched M~^+M~ of 1, 2 and 4 (timed once, then cached).  The
 // register-blocked passes need h = 0.  ms: the chosen time, when timed.
 int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* ms) {
   int& cached = c->tuned_nbt[(int)p][nb];
@@ -622,7 +659,7 @@ int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* 
   for (int k : {1, 2, 4}) {
     if (k > 1 && (k > nb || op.h != 0.0 || p == Prec::F64 || c->g.clover_t)) break;
     float t;
-    int st = time_pass1(c, p, op, nb, k, 3, &t);
+    int st = time_mdagm_batch(c, p, op, nb, k, 2, &t);
     if (st) return st;
     if (k == 1 || t < 0.98f * best) {
       best = t;
@@ -635,9 +672,9 @@ int tune_nbt(bqcdg_ctx* c, Prec p, const OpParams& op, int nb, int* nbt, float* 
   return BQCDG_OK;
 }
 
-// RHS per launch for a batch: the per-RHS time of the first stencil pass
-// (at its best RHS per thread), timed for 1, 4, 8 and 16 right-hand sides
-// on the resident fields
+// RHS per launch for a batch: the per-RHS time of a batched M~^+M~ (at its
+// best RHS per thread), timed for 1, 4, 8 and 16 right-hand sides on the
+// resident fields
 int tune_block(bqcdg_ctx* c, Prec p, const OpParams& op, int nmax, int* best) {
   const int cand[4] = {1, 4, 8, 16};
   int cap = 1;

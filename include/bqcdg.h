@@ -79,7 +79,9 @@ typedef struct {
   double tol;
   double delta;       /* reliable update when |r| < delta * max|r| since the last one */
   int check_true_residual; /* 1: recompute |b - A x|^2 in FP64 at the end */
-  int time_kernels;   /* 1: time every stencil launch with CUDA events */
+  int time_kernels;   /* 1: time the first-half stencil launches of the first
+                         iteration of every batch of queued iterations with
+                         CUDA events (FP64 and single-RHS sloppy solves) */
   int rhs_per_thread; /* batched solves: right-hand sides each stencil thread serves
                          (1, 2, 4; 0 = the fastest, timed once per context) */
 } bqcdg_solver_opts;
@@ -91,8 +93,9 @@ typedef struct {
   double true_rtr;        /* final |b - A x|^2 in FP64 (if checked) */
   double b2;              /* |b|^2 */
   double seconds;         /* device time of the solve (CUDA events) */
-  double stencil_ms;      /* summed device time of the dominant stencil kernel */
-  int stencil_launches;   /* launches of that kernel */
+  double stencil_ms;      /* summed device time of the timed launches of the
+                             dominant stencil kernel (time_kernels) */
+  int stencil_launches;   /* how many launches were timed */
   int converged;
   int kernel_launches;    /* all kernels this solve launched */
 } bqcdg_solve_info;
