@@ -12,6 +12,13 @@
 //          slab's stream.  libnccl.so.2 is opened at run time (the one a
 //          process such as PyTorch has loaded already, if any).
 //
+// Every stencil pass overlaps the exchange with the slab's interior: the
+// faces are packed and sent on an exchange stream (xstream) as soon as the
+// input field is ready, the interior slices 1 .. Lt_loc-2, which read no
+// ghost, run meanwhile on the compute stream, and the two boundary slices
+// run after the exchange (an event).  Each site's arithmetic is that of one
+// whole-slab launch, so the split changes no result.
+//
 // The reference does the same over MPI: project to half spinors
 // (d/D21.F90:53), exchange the faces (xbound, comm/xbound_mpi.F90:418-461),
 // compute (d/D21.F90:58-72), and global_sum the CG scalars (cg.F90:91,97,109).
@@ -27,10 +34,11 @@ void launch_dd_pack(const Geom& g, const DdGeom& d, bool dag, const double2* in,
 void launch_dd_pack_links(const Geom& g, const DdGeom& d, const double2* gauge, double2* to_next, cudaStream_t s);
 void launch_dd_dslash(const Geom& g, const DdGeom& d, int e, bool dag, double2* out, const double2* in,
                       const double2* gauge, cudaStream_t s);
+// part: 0 the whole slab, 1 its interior slices, 2 its boundary slices (dd_part_sites)
 void launch_dd_pass1(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* in, const double2* gauge,
-                     const double2* ainv, const OpParams& op, cudaStream_t s);
+                     const double2* ainv, const OpParams& op, cudaStream_t s, int part);
 void launch_dd_pass2(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* t, const double2* in,
-                     const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s);
+                     const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s, int part);
 }  // namespace bqcdg
 
 using namespace bqcdg_host;
@@ -85,7 +93,10 @@ struct bqcdg_dd {
   int Lt_loc = 0, V3h = 0, volh_loc = 0;
   std::vector<bqcdg_ctx*> slabs;
   std::vector<SlabBufs> bufs;
-  cudaStream_t stream = nullptr;  // every slab works on the first slab's stream
+  cudaStream_t stream = nullptr;  // every slab computes on the first slab's stream
+  cudaStream_t xstream = nullptr; // face packing and exchange
+  cudaEvent_t ev_ready = nullptr; // on stream: the field to exchange is written
+  cudaEvent_t ev_done = nullptr;  // on xstream: the ghosts are filled
   ncclComm_t comm = nullptr;
   double* dsum = nullptr;         // nccl: device scalars of the global sums
   std::vector<double> hsum;
@@ -111,29 +122,39 @@ namespace {
 int dd_check(bqcdg_dd* dd) { return dd && !dd->slabs.empty() ? BQCDG_OK : BQCDG_EINVAL; }
 
 // the faces of field f[s] of every slab, for passes with (dag) or without
-// the dagger, into the ghost buffers of their neighbours
+// the dagger, into the ghost buffers of their neighbours: queued on xstream
+// after everything queued so far on the compute stream (which includes the
+// last reads of the ghosts this overwrites); dd_wait_exchange makes the
+// compute stream wait for it
 int dd_exchange(bqcdg_dd* dd, const std::vector<double2*>& f, bool dag) {
   const int n = dd->nslabs();
+  CK(cudaEventRecord(dd->ev_ready, dd->stream));
+  CK(cudaStreamWaitEvent(dd->xstream, dd->ev_ready, 0));
   if (!dd->nccl) {
     for (int s = 0; s < n; s++) {
       const int prev = (s + n - 1) % n, next = (s + 1) % n;
       launch_dd_pack(dd->slabs[s]->g, dd->geom(s), dag, f[s], dd->bufs[prev].ghost_fwd, dd->bufs[next].ghost_bwd,
-                     dd->stream);
+                     dd->xstream);
     }
     CKL();
-    return BQCDG_OK;
+  } else {
+    SlabBufs& b = dd->bufs[0];
+    launch_dd_pack(dd->slabs[0]->g, dd->geom(0), dag, f[0], b.send_prev, b.send_next, dd->xstream);
+    CKL();
+    const int r = dd->rank0, prev = (r + dd->nranks - 1) % dd->nranks, next = (r + 1) % dd->nranks;
+    const size_t cnt = (size_t)6 * dd->V3h * 2;  // doubles per face
+    if (g_nccl.groupStart() != ncclSuccess) return BQCDG_ECUDA;
+    ncclResult_t e = g_nccl.send(b.send_prev, cnt, ncclDouble, prev, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.recv(b.ghost_fwd, cnt, ncclDouble, next, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.send(b.send_next, cnt, ncclDouble, next, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclDouble, prev, dd->comm, dd->xstream);
+    if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
   }
-  SlabBufs& b = dd->bufs[0];
-  launch_dd_pack(dd->slabs[0]->g, dd->geom(0), dag, f[0], b.send_prev, b.send_next, dd->stream);
-  CKL();
-  const int r = dd->rank0, prev = (r + dd->nranks - 1) % dd->nranks, next = (r + 1) % dd->nranks;
-  const size_t cnt = (size_t)6 * dd->V3h * 2;  // doubles per face
-  if (g_nccl.groupStart() != ncclSuccess) return BQCDG_ECUDA;
-  ncclResult_t e = g_nccl.send(b.send_prev, cnt, ncclDouble, prev, dd->comm, dd->stream);
-  if (e == ncclSuccess) e = g_nccl.recv(b.ghost_fwd, cnt, ncclDouble, next, dd->comm, dd->stream);
-  if (e == ncclSuccess) e = g_nccl.send(b.send_next, cnt, ncclDouble, next, dd->comm, dd->stream);
-  if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclDouble, prev, dd->comm, dd->stream);
-  if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
+  CK(cudaEventRecord(dd->ev_done, dd->xstream));
+  return BQCDG_OK;
+}
+int dd_wait_exchange(bqcdg_dd* dd) {
+  CK(cudaStreamWaitEvent(dd->stream, dd->ev_done, 0));
   return BQCDG_OK;
 }
 
@@ -188,15 +209,22 @@ int dd_mtil(bqcdg_dd* dd, bool dag, const std::vector<double2*>& out, const std:
             const std::vector<double2*>& t, const OpParams& op) {
   int st;
   if ((st = dd_exchange(dd, in, dag))) return st;
-  for (int s = 0; s < dd->nslabs(); s++) {
-    bqcdg_ctx* c = dd->slabs[s];
-    launch_dd_pass1(c->g, dd->geom(s), dag, t[s], in[s], c->gauge64, ainv_oo_of_slab(c), op, dd->stream);
+  for (int part = 1; part <= 2; part++) {  // interior while the faces travel, then the boundary slices
+    if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+    for (int s = 0; s < dd->nslabs(); s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_dd_pass1(c->g, dd->geom(s), dag, t[s], in[s], c->gauge64, ainv_oo_of_slab(c), op, dd->stream, part);
+    }
   }
   CKL();
   if ((st = dd_exchange(dd, t, dag))) return st;
-  for (int s = 0; s < dd->nslabs(); s++) {
-    bqcdg_ctx* c = dd->slabs[s];
-    launch_dd_pass2(c->g, dd->geom(s), dag, out[s], t[s], in[s], c->gauge64, aee_of_slab(c), op, dd->stream);
+  for (int part = 1; part <= 2; part++) {
+    if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+    for (int s = 0; s < dd->nslabs(); s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_dd_pass2(c->g, dd->geom(s), dag, out[s], t[s], in[s], c->gauge64, aee_of_slab(c), op, dd->stream,
+                      part);
+    }
   }
   CKL();
   return BQCDG_OK;
@@ -264,6 +292,14 @@ int dd_create(bqcdg_dd** out, const int L[4], const int bc[4], int nranks, int r
     dd->bufs.push_back(SlabBufs{});
   }
   dd->stream = dd->slabs[0]->stream;
+  cudaError_t es = cudaSetDevice(device);
+  if (es == cudaSuccess) es = cudaStreamCreateWithFlags(&dd->xstream, cudaStreamNonBlocking);
+  if (es == cudaSuccess) es = cudaEventCreateWithFlags(&dd->ev_ready, cudaEventDisableTiming);
+  if (es == cudaSuccess) es = cudaEventCreateWithFlags(&dd->ev_done, cudaEventDisableTiming);
+  if (es != cudaSuccess) {
+    bqcdg_dd_destroy(dd);
+    return status_from_cuda(es);
+  }
   const size_t face = (size_t)6 * dd->V3h * sizeof(double2), links = (size_t)18 * dd->V3h * sizeof(double2);
   for (int s = 0; s < nslabs; s++) {
     bqcdg_ctx* c = dd->slabs[s];
@@ -326,6 +362,10 @@ int bqcdg_dd_create_nccl(bqcdg_dd** out, const int L[4], const int bc[4], int nr
 int bqcdg_dd_destroy(bqcdg_dd* dd) {
   if (!dd) return BQCDG_EINVAL;
   if (dd->comm) g_nccl.commDestroy(dd->comm);
+  if (dd->xstream) cudaStreamSynchronize(dd->xstream);
+  if (dd->ev_ready) cudaEventDestroy(dd->ev_ready);
+  if (dd->ev_done) cudaEventDestroy(dd->ev_done);
+  if (dd->xstream) cudaStreamDestroy(dd->xstream);
   for (bqcdg_ctx* c : dd->slabs) bqcdg_destroy(c);  // frees every buffer the slab allocated
   delete dd;
   return BQCDG_OK;
@@ -387,7 +427,7 @@ int bqcdg_dd_op(bqcdg_dd* dd, int which, double* out, const double* in, const bq
     case 1: case 4: st = dd_mtil(dd, true, vout, vin, t, op); break;
     case 2: case 5: st = dd_mdagm(dd, vout, vin, t, q, op); break;
     default:  // 6: d(EVEN, ODD), 7: d_dag(EVEN, ODD)
-      if ((st = dd_exchange(dd, vin, which == 7))) break;
+      if ((st = dd_exchange(dd, vin, which == 7)) || (st = dd_wait_exchange(dd))) break;
       for (int s = 0; s < dd->nslabs(); s++)
         launch_dd_dslash(dd->slabs[s]->g, dd->geom(s), 0, which == 7, vout[s], vin[s], dd->slabs[s]->gauge64,
                          dd->stream);

@@ -96,10 +96,11 @@ __global__ void __launch_bounds__(kBlock) k_dd_dslash(Geom g, DdGeom d, int e, d
 
 // t_o = [(1 -+ i h g5)] A_oo^-1 D_oe in_e (m_tilde.F90:55-58, 92-95)
 template <bool DAG>
-__global__ void __launch_bounds__(kBlock) k_dd_pass1(Geom g, DdGeom d, double2* out, const double2* in,
+__global__ void __launch_bounds__(kBlock) k_dd_pass1(Geom g, DdGeom d, int part, double2* out, const double2* in,
                                                      const double2* gauge, const double2* ainv, double hval) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.volh) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= dd_part_sites(part, g.L[3], d.V3h)) return;
+  const int i = dd_part_site(part, g.L[3], d.V3h, j);
   SpinorView<Prec::F64> IN{(double2*)in, g.stride}, OUT{out, g.stride};
   GaugeView<Prec::F64> U{(double2*)gauge, g.stride, 0};
   const Site st = site_coords(g, i, 1);
@@ -119,11 +120,12 @@ __global__ void __launch_bounds__(kBlock) k_dd_pass1(Geom g, DdGeom d, double2* 
 // + rho x (m_tilde.F90:63-73, w_mult.F90:39): the site-local terms first,
 // as in pass2_core
 template <bool DAG>
-__global__ void __launch_bounds__(kBlock) k_dd_pass2(Geom g, DdGeom d, double2* out, const double2* tin,
+__global__ void __launch_bounds__(kBlock) k_dd_pass2(Geom g, DdGeom d, int part, double2* out, const double2* tin,
                                                      const double2* xin, const double2* gauge, const double2* aee,
                                                      double bcoef, double hval, double rho) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.volh) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= dd_part_sites(part, g.L[3], d.V3h)) return;
+  const int i = dd_part_site(part, g.L[3], d.V3h, j);
   SpinorView<Prec::F64> T{(double2*)tin, g.stride}, X{(double2*)xin, g.stride}, OUT{out, g.stride};
   GaugeView<Prec::F64> U{(double2*)gauge, g.stride, 0};
   Spinor<double> x, o;
@@ -199,19 +201,23 @@ void launch_dd_dslash(const Geom& g, const DdGeom& d, int e, bool dag, double2* 
   else k_dd_dslash<false><<<nblocks(g.volh), kBlock, 0, s>>>(g, d, e, out, in, gauge);
 }
 void launch_dd_pass1(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* in, const double2* gauge,
-                     const double2* ainv, const OpParams& op, cudaStream_t s) {
+                     const double2* ainv, const OpParams& op, cudaStream_t s, int part) {
+  const int n = dd_part_sites(part, g.L[3], d.V3h);
+  if (n <= 0) return;  // no interior in a slab of two slices
   const double hv = dag ? op.h : -op.h;
   const double2* ai = op.csw_kappa != 0.0 ? ainv : nullptr;
-  if (dag) k_dd_pass1<true><<<nblocks(g.volh), kBlock, 0, s>>>(g, d, out, in, gauge, ai, hv);
-  else k_dd_pass1<false><<<nblocks(g.volh), kBlock, 0, s>>>(g, d, out, in, gauge, ai, hv);
+  if (dag) k_dd_pass1<true><<<nblocks(n), kBlock, 0, s>>>(g, d, part, out, in, gauge, ai, hv);
+  else k_dd_pass1<false><<<nblocks(n), kBlock, 0, s>>>(g, d, part, out, in, gauge, ai, hv);
 }
 void launch_dd_pass2(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* t, const double2* in,
-                     const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s) {
+                     const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s, int part) {
+  const int n = dd_part_sites(part, g.L[3], d.V3h);
+  if (n <= 0) return;
   const double bcoef = -op.kappa * op.kappa / (1.0 + op.h * op.h);
   const double hv = dag ? -op.h : op.h;
   const double2* a = op.csw_kappa != 0.0 ? aee : nullptr;
-  if (dag) k_dd_pass2<true><<<nblocks(g.volh), kBlock, 0, s>>>(g, d, out, t, in, gauge, a, bcoef, hv, op.rho);
-  else k_dd_pass2<false><<<nblocks(g.volh), kBlock, 0, s>>>(g, d, out, t, in, gauge, a, bcoef, hv, op.rho);
+  if (dag) k_dd_pass2<true><<<nblocks(n), kBlock, 0, s>>>(g, d, part, out, t, in, gauge, a, bcoef, hv, op.rho);
+  else k_dd_pass2<false><<<nblocks(n), kBlock, 0, s>>>(g, d, part, out, t, in, gauge, a, bcoef, hv, op.rho);
 }
 
 }  // namespace bqcdg

@@ -73,4 +73,18 @@ __host__ __device__ __forceinline__ int dd_tneighbour(const Geom& g, const DdGeo
   return t == 0 ? -1 - i : i - d.V3h;
 }
 
+// Overlap of the exchange with the slab's interior: a pass runs as two
+// launches, the interior slices 1 .. Lt_loc-2 (no ghost read) while the faces
+// travel, then the boundary slices 0 and Lt_loc-1.  dd_part_sites: sites of
+// part (0 all, 1 interior, 2 boundary); dd_part_site: the local site of
+// thread j (0 <= j < dd_part_sites) of that part.
+__host__ __device__ __forceinline__ int dd_part_sites(int part, int Lt_loc, int V3h) {
+  return part == 0 ? Lt_loc * V3h : (part == 1 ? (Lt_loc - 2) * V3h : 2 * V3h);
+}
+__host__ __device__ __forceinline__ int dd_part_site(int part, int Lt_loc, int V3h, int j) {
+  if (part == 1) return V3h + j;
+  if (part == 2) return j < V3h ? j : (Lt_loc - 1) * V3h + (j - V3h);
+  return j;
+}
+
 }  // namespace bqcdg

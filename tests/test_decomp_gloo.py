@@ -171,3 +171,15 @@ def test_gloo_slabs_equal_the_single_domain_operator(tmp_path, world, L, dag):
         assert p.exitcode == 0
     assert sorted(res) == list(range(world))
     assert max(res.values()) < 1e-13, res
+
+
+def test_interior_and_boundary_launches_partition_the_slab(tmp_path):
+    """A slab pass runs as an interior launch (slices 1 .. Lt_loc-2, while the
+    faces are exchanged) and a boundary launch (slices 0 and Lt_loc-1): every
+    site in exactly one of them, no interior site reading a ghost, every
+    boundary site reading one (tests/c_client/dd_parts.cu over decomp.cuh)."""
+    exe = os.path.join(str(tmp_path), "dd_parts")
+    subprocess.run([os.environ.get("NVCC", "nvcc"), "-std=c++17", "-O1", "-o", exe,
+                    os.path.join(ROOT, "tests", "c_client", "dd_parts.cu")], check=True, capture_output=True)
+    r = subprocess.run([exe, "8,8,8,2", "8,8,8,4", "4,6,4,6", "6,4,6,12", "2,2,2,8"], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
