@@ -310,15 +310,33 @@ class Hmc:
         sg = lat.sg()
         return sd + lat.mom_action() + sg * self.beta + sf1 + sf2, sg
 
-    def trajectory(self, force_accept=False):
-        """hmc.F90:69-216: one trajectory; returns its record as a dict."""
-        lat = self.lat
+    def _reset_stats(self):
         self.cg_ncall = self.cg_niter_tot = self.cg_niter_max = 0
         self.cg_seconds = 0.0
         self.it_f1 = self.it_f2 = 0
         self.f_count = [0.0] * 4
         self.f_avg = [0.0] * 4
         self.f_max = [0.0] * 4
+
+    def init_phi(self):
+        """New pseudofermions on the current links (hmc_init_phi.F90);
+        returns their actions (S_f1, S_f2)."""
+        self._reset_stats()
+        return self._init_phi()
+
+    def md_evolve(self):
+        """The molecular-dynamics part of a trajectory alone: the nested
+        leapfrog from the current links and momenta with the pseudofermions
+        fixed; returns the fermion actions (S_f1, S_f2) at the end."""
+        self._reset_stats()
+        self.sf1 = self.sf2 = 0.0
+        self._leap_frog()
+        return self.sf1, self.sf2
+
+    def trajectory(self, force_accept=False):
+        """hmc.F90:69-216: one trajectory; returns its record as a dict."""
+        lat = self.lat
+        self._reset_stats()
         lat.gauge_save()
         lat.field_copy(self.phi_bck, self.phi)
         lat.mom_gauss()

@@ -235,3 +235,44 @@ def test_mpp_benchmark_job_on_device(bq):
         assert lat.ranget() == gold["final_seed"]
     finally:
         lat.close()
+
+
+@pytest.mark.parametrize("solver", ["cg", "mixed"])
+def test_leapfrog_is_reversible(bq, solver):
+    """The nested leapfrog (hmc_leap_frog.F90) with the device forces is
+    reversible: integrate a model-C system (Hasenbusch, clover) forward,
+    negate the momenta and integrate again, and the links and momenta return
+    to their start, to the accuracy of the solves (the MRE guesses differ
+    between the two legs, so each solve contributes its tolerance); the
+    fermion and gauge actions, and so H, return with them.  A leapfrog that
+    is not reversible, or a force that is not the gradient of the action it
+    is paired with, leaves an O(step^2) difference."""
+    from bqcdg.hmc import Hmc, quenched_trajectory
+    with bq.Lattice((8, 8, 8, 8), BC) as lat:
+        lat.ranset(5)
+        lat.conf_hot()
+        lat.conf_relax(2)
+        for _ in range(3):
+            quenched_trajectory(lat, 5.29, 1.0, 20, force_accept=True)
+        rest = 1e-24 * 12 * 2 * lat.volh   # |r|/|b| about 1e-12 for these pseudofermions
+        hmc = Hmc(lat, beta=5.29, kappa=0.13, csw=1.9192, rho=0.1, traj_length=0.5, ntau=5, m_scale=2, model="C",
+                  rest=rest, maxiter=20000, solver=solver)
+        lat.mom_gauss()
+        sf0 = hmc.init_phi()
+        u0, p0 = lat.get_gauge(), lat.mom_get()
+        h0 = lat.mom_action() + 5.29 * lat.sg() + sum(sf0)
+        hmc.md_evolve()
+        u1 = lat.get_gauge()
+        lat.mom_set(-lat.mom_get())
+        sf2 = hmc.md_evolve()
+        u2, p2 = lat.get_gauge(), lat.mom_get()
+        h2 = lat.mom_action() + 5.29 * lat.sg() + sum(sf2)
+        moved = np.linalg.norm(u1 - u0) / np.linalg.norm(u0)
+        du = np.linalg.norm(u2 - u0) / np.linalg.norm(u0)
+        dp = np.linalg.norm(p2 + p0) / np.linalg.norm(p0)
+        print("reversibility (%s): links moved %.2e, back to %.2e; momenta %.2e; H %.6e -> %.6e"
+              % (solver, moved, du, dp, h0, h2))
+        assert moved > 1e-3
+        tol = 1e-9 if solver == "cg" else 1e-6
+        assert du < tol and dp < tol
+        assert abs(h2 - h0) < (1e-6 if solver == "cg" else 1e-3) * abs(h0)
