@@ -301,7 +301,7 @@ def run_ours(args):
 
     if rank == 0:
         it = infos[-1]
-        flops_site_iter = 4 * 1824          # 4 clover D-slash applications per M^+M (north_star convention)
+        flops_site_iter = 4 * 1824          # 4 clover D-slash applications per M^+M, 1824 flop each
         gflops = flops_site_iter * lat.volh * it.niter / step_s / 1e9
         out = {
             "metric": METRIC,
