@@ -168,6 +168,7 @@ def _lib_handle():
         L.bqcdg_dd_load_clover.argtypes = [vp, dp, dp]
         L.bqcdg_dd_op.argtypes = [vp, i, dp, dp, P(Params)]
         L.bqcdg_dd_cg.argtypes = [vp, dp, dp, P(Params), P(CgPara), P(C.c_int), P(SolveInfo)]
+        L.bqcdg_dd_solve.argtypes = [vp, dp, dp, P(Params), P(SolverOpts), P(SolveInfo)]
         _LIB = L
     return _LIB
 
@@ -672,7 +673,8 @@ class Lattice:
 
 
 class SlabDecomposition:
-    """The lattice cut along t into nranks slabs (bqcdg_dd_* of bqcdg.h), FP64.
+    """The lattice cut along t into nranks slabs (bqcdg_dd_* of bqcdg.h): the
+    FP64 operators and CG, and the mixed-precision solve (solve).
 
     SlabDecomposition.local(L, nranks): every slab in this process on one
     device (host arrays are the global ones).  SlabDecomposition.nccl(L,
@@ -743,3 +745,16 @@ class SlabDecomposition:
         _check(lib().bqcdg_dd_cg(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(cp),
                                  C.byref(it), C.byref(info)), "dd_cg")
         return x, it.value, info
+
+    def solve(self, x, b, para, tol=1e-10, relative=True, maxiter=100000, delta=0.1, rho=None):
+        """bqcdg_dd_solve: int16 iterations with FP64 reliable updates;
+        returns (x, info).  No convergence is reported in info, not raised."""
+        x = np.array(x, dtype=np.complex128, copy=True, order="C")
+        info = SolveInfo()
+        prm = para.params(rho) if isinstance(para, HmcPara) else para
+        o = SolverOpts(PREC_HALF, maxiter, int(relative), tol, delta, 1, 0)
+        st = lib().bqcdg_dd_solve(self.h, x.ctypes.data, _ptr(b, np.complex128), C.byref(prm), C.byref(o),
+                                  C.byref(info))
+        if st not in (OK, ENOCONV):
+            _check(st, "dd_solve")
+        return x, info

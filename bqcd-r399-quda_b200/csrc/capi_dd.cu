@@ -39,6 +39,21 @@ void launch_dd_pass1(const Geom& g, const DdGeom& d, bool dag, double2* out, con
                      const double2* ainv, const OpParams& op, cudaStream_t s, int part);
 void launch_dd_pass2(const Geom& g, const DdGeom& d, bool dag, double2* out, const double2* t, const double2* in,
                      const double2* gauge, const double2* aee, const OpParams& op, cudaStream_t s, int part);
+// int16 slab passes (decomp16.cu); the second halves return the number of
+// blocks whose partials they stored from slot0 on
+void launch_dd16_pack(const Geom& g, const DdGeom& d, bool dag, SpinorPtr in, float2* to_prev, float2* to_next,
+                      cudaStream_t s);
+void launch_dd16_pass1(const Geom& g, const DdGeom& d, bool dag, int part, SpinorPtr out, SpinorPtr in,
+                       const void* gauge, CloverPtr ainv, const OpParams& op, const CgScalars* cg, cudaStream_t s);
+int launch_dd16_pass2(const Geom& g, const DdGeom& d, bool dag, int part, SpinorPtr out, SpinorPtr t, SpinorPtr x,
+                      const void* gauge, CloverPtr aee, const OpParams& op, double* partial, int slot0,
+                      const CgScalars* cg, cudaStream_t s);
+int launch_dd16_pass4(const Geom& g, const DdGeom& d, int part, SpinorPtr t, SpinorPtr q, const void* gauge,
+                      CloverPtr aee, const OpParams& op, SpinorPtr r, double* partial, int slot0, const CgScalars* cg,
+                      cudaStream_t s);
+void launch_dd_total(const DdPartials& parts, int nslabs, int nsb, CgScalars* cg, double* out, int mode,
+                     cudaStream_t s);
+void launch_dd_apply(const double* tot, CgScalars* cg, int mode, cudaStream_t s);
 }  // namespace bqcdg
 
 using namespace bqcdg_host;
@@ -99,6 +114,7 @@ struct bqcdg_dd {
   cudaEvent_t ev_done = nullptr;  // on xstream: the ghosts are filled
   ncclComm_t comm = nullptr;
   double* dsum = nullptr;         // nccl: device scalars of the global sums
+  double* dtot = nullptr;         // the mixed solver's reduction total
   std::vector<double> hsum;
 
   int nslabs() const { return (int)slabs.size(); }
@@ -155,6 +171,58 @@ int dd_exchange(bqcdg_dd* dd, const std::vector<double2*>& f, bool dag) {
 }
 int dd_wait_exchange(bqcdg_dd* dd) {
   CK(cudaStreamWaitEvent(dd->stream, dd->ev_done, 0));
+  return BQCDG_OK;
+}
+
+// dd_exchange for an int16 field: FP32 faces (half the bytes of the FP64
+// ones) in the same ghost and send buffers
+int dd_exchange16(bqcdg_dd* dd, const std::vector<SpinorPtr>& f, bool dag) {
+  const int n = dd->nslabs();
+  CK(cudaEventRecord(dd->ev_ready, dd->stream));
+  CK(cudaStreamWaitEvent(dd->xstream, dd->ev_ready, 0));
+  if (!dd->nccl) {
+    for (int s = 0; s < n; s++) {
+      const int prev = (s + n - 1) % n, next = (s + 1) % n;
+      launch_dd16_pack(dd->slabs[s]->g, dd->geom(s), dag, f[s], (float2*)dd->bufs[prev].ghost_fwd,
+                       (float2*)dd->bufs[next].ghost_bwd, dd->xstream);
+    }
+    CKL();
+  } else {
+    SlabBufs& b = dd->bufs[0];
+    launch_dd16_pack(dd->slabs[0]->g, dd->geom(0), dag, f[0], (float2*)b.send_prev, (float2*)b.send_next,
+                     dd->xstream);
+    CKL();
+    const int r = dd->rank0, prev = (r + dd->nranks - 1) % dd->nranks, next = (r + 1) % dd->nranks;
+    const size_t cnt = (size_t)6 * dd->V3h * 2;  // floats per face
+    if (g_nccl.groupStart() != ncclSuccess) return BQCDG_ECUDA;
+    ncclResult_t e = g_nccl.send(b.send_prev, cnt, ncclFloat, prev, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.recv(b.ghost_fwd, cnt, ncclFloat, next, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.send(b.send_next, cnt, ncclFloat, next, dd->comm, dd->xstream);
+    if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclFloat, prev, dd->comm, dd->xstream);
+    if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
+  }
+  CK(cudaEventRecord(dd->ev_done, dd->xstream));
+  return BQCDG_OK;
+}
+
+// the reduction over all slabs of the partials the last second pass stored
+// (nsb per slab, from slot 0 of each slab's RedScratch), applied by mode
+// (1: alpha, 2: the CG step) to the shared scalars: in this process in slab
+// order, then over the ranks by ncclAllReduce
+int dd_reduce(bqcdg_dd* dd, int nsb, CgScalars* cg, int mode) {
+  DdPartials parts{};
+  for (int s = 0; s < dd->nslabs(); s++) parts.p[s] = dd->slabs[s]->red.partial;
+  if (!dd->nccl) {
+    launch_dd_total(parts, dd->nslabs(), nsb, cg, nullptr, mode, dd->stream);
+    CKL();
+    return BQCDG_OK;
+  }
+  launch_dd_total(parts, dd->nslabs(), nsb, cg, dd->dtot, 0, dd->stream);
+  CKL();
+  if (g_nccl.allReduce(dd->dtot, dd->dtot, 1, ncclDouble, ncclSum, dd->comm, dd->stream) != ncclSuccess)
+    return BQCDG_ECUDA;
+  launch_dd_apply(dd->dtot, cg, mode, dd->stream);
+  CKL();
   return BQCDG_OK;
 }
 
@@ -307,6 +375,7 @@ int dd_create(bqcdg_dd** out, const int L[4], const int bc[4], int nranks, int r
     cudaError_t e = c->alloc((void**)&b.ghost_fwd, face);
     if (e == cudaSuccess) e = c->alloc((void**)&b.ghost_bwd, face);
     if (e == cudaSuccess) e = c->alloc((void**)&b.ghost_link, links);
+    if (e == cudaSuccess && s == 0) e = c->alloc((void**)&dd->dtot, 4 * sizeof(double));
     if (e != cudaSuccess) {
       bqcdg_dd_destroy(dd);
       return status_from_cuda(e);
@@ -521,6 +590,208 @@ int bqcdg_dd_cg(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p,
   if (iterations) *iterations = niter;
   if (!(rtr == rtr)) return BQCDG_ENAN;
   if (!conv && cgp->log != 2) return BQCDG_ENOCONV;
+  return BQCDG_OK;
+}
+
+// The mixed-precision solve over the slabs: the scheme of cg_core (capi.cu)
+// -- int16 sloppy iterations, FP32 r and x_s, FP64 reliable updates when |r|
+// has fallen by o->delta, p re-orthogonalised after each -- with every
+// stencil pass split around the face exchange and the two reductions of an
+// iteration summed over all slabs (dd_reduce) into one set of CG scalars on
+// the device, so the iterations never wait for the host.
+int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p, const bqcdg_solver_opts* o,
+                   bqcdg_solve_info* info) {
+  int st = dd_check(dd);
+  if (st || !x || !b || !p || !o || !info) return BQCDG_EINVAL;
+  if (o->precision != BQCDG_PREC_HALF) return BQCDG_EUNSUPPORTED;  // FP64: bqcdg_dd_cg
+  if (dd->nslabs() > kMaxDdSlabs || o->delta <= 0.0 || o->delta >= 1.0) return BQCDG_EINVAL;
+  const bool clover = p->csw_kappa != 0.0;
+  for (bqcdg_ctx* c : dd->slabs) {
+    if (!c->have_gauge) return BQCDG_ENOGAUGE;
+    if (clover && (!c->have_A[0] || !c->have_Ainv[1])) return BQCDG_ENOCLOVER;
+  }
+  CK(cudaSetDevice(dd->slabs[0]->device));
+  std::memset(info, 0, sizeof(*info));
+  const int n = dd->nslabs();
+  const Prec P = Prec::F16;
+  for (bqcdg_ctx* c : dd->slabs)
+    if ((st = ensure_sloppy(c, P, clover))) return st;
+  std::vector<double2*> vx, vb, vr, vax, t64, q64;
+  if ((st = dd_fields(dd, 0, vx)) || (st = dd_fields(dd, 1, vb)) || (st = dd_fields(dd, 2, vr)) ||
+      (st = dd_fields(dd, 3, vax)) || (st = dd_fields(dd, 4, t64)) || (st = dd_fields(dd, 5, q64)))
+    return st;
+  std::vector<SpinorPtr> sp(n), st_(n), sq(n), rs(n), xs(n);
+  for (int s = 0; s < n; s++) {
+    bqcdg_ctx* c = dd->slabs[s];
+    sp[s] = c->sp(P, 0);
+    st_[s] = c->sp(P, 1);
+    sq[s] = c->sp(P, 2);
+    rs[s] = c->sp(Prec::F32, 0);
+    xs[s] = c->sp(Prec::F32, 1);
+    if (!sp[s].v || !st_[s].v || !sq[s].v || !rs[s].v || !xs[s].v) return BQCDG_ENOMEM;
+  }
+  if ((st = dd_upload(dd, x, vx)) || (st = dd_upload(dd, b, vb))) return st;
+  const OpParams op = op_of(p, true);
+  bqcdg_ctx* c0 = dd->slabs[0];
+  CgScalars* dcg = c0->dcg;  // the scalars every slab's kernels read
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, dd->stream));
+
+  // r = b - A x in FP64 and |r|^2, |b|^2 over the slabs
+  auto residual = [&](double* r2b2) -> int {
+    int s2 = dd_mdagm(dd, vax, vx, t64, q64, op);
+    if (s2) return s2;
+    for (int s = 0; s < n; s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_residual(c->g, vr[s], vb[s], vax[s], Prec::F32, rs[s], c->red, c->dres, dd->stream);
+    }
+    CKL();
+    return dd_global_sum(dd, 2, r2b2);
+  };
+  double rb[2];
+  if ((st = residual(rb))) return st;
+  const double b2 = rb[1];
+  const double stop = o->relative ? o->tol * o->tol * b2 : o->tol;
+  info->b2 = b2;
+  for (int s = 0; s < n; s++) {
+    launch_spinor_convert(dd->slabs[s]->g, P, sp[s], Prec::F32, rs[s], dd->stream);
+    launch_zero(dd->slabs[s]->g, Prec::F32, xs[s], dd->stream);
+  }
+  CKL();
+  CgScalars h{};
+  h.rtr = h.rtr_old = rb[0];
+  h.stop_rtr = stop;
+  h.maxiter = o->maxiter;
+  h.delta2 = o->delta * o->delta;
+  h.maxr2 = rb[0];
+  h.ru_every = 500;  // periodic reliable updates of the int16 iterations, as in cg_core
+  bool converged = false;
+  if (!(rb[0] == rb[0])) h.done = 4;
+  else if (rb[0] == 0.0 || rb[0] <= stop) { h.done = 1; converged = true; }
+  if (o->maxiter <= 0 && !h.done) h.done = 3;
+  auto put = [&]() -> int {
+    CK(cudaMemcpyAsync(dcg, &h, sizeof(h), cudaMemcpyHostToDevice, dd->stream));
+    CK(cudaStreamSynchronize(dd->stream));
+    return BQCDG_OK;
+  };
+  auto get = [&]() -> int {
+    CK(cudaMemcpyAsync(&h, dcg, sizeof(h), cudaMemcpyDeviceToHost, dd->stream));
+    CK(cudaStreamSynchronize(dd->stream));
+    return BQCDG_OK;
+  };
+  if ((st = put())) return st;
+  const int nsb1 = nblocks(dd_part_sites(1, dd->Lt_loc, dd->V3h));
+  const int nsb = nsb1 + nblocks(dd_part_sites(2, dd->Lt_loc, dd->V3h));
+  int batch = 4, ru = 0, stall = 0, forced = 0, launches = 0;
+  double best = rb[0];
+  bool stalled = false;
+  while (!h.done) {
+    const int iter0 = h.iter;
+    for (int k = 0; k < batch; k++) {
+      // pass 1: t = A_oo^-1 D_oe p
+      if ((st = dd_exchange16(dd, sp, false))) return st;
+      for (int part = 1; part <= 2; part++) {
+        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+        for (int s = 0; s < n; s++) {
+          bqcdg_ctx* c = dd->slabs[s];
+          launch_dd16_pass1(c->g, dd->geom(s), false, part, st_[s], sp[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+                            dd->stream);
+        }
+      }
+      // pass 2: q = M~ p, |q|^2 -> alpha
+      if ((st = dd_exchange16(dd, st_, false))) return st;
+      for (int part = 1; part <= 2; part++) {
+        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+        for (int s = 0; s < n; s++) {
+          bqcdg_ctx* c = dd->slabs[s];
+          launch_dd16_pass2(c->g, dd->geom(s), false, part, sq[s], st_[s], sp[s], gauge_of(c, P), aee_of(c, P), op,
+                            c->red.partial, part == 1 ? 0 : nsb1, dcg, dd->stream);
+        }
+      }
+      CKL();
+      if ((st = dd_reduce(dd, nsb, dcg, 1))) return st;
+      // pass 3: t = A_oo^-1 D^+_oe q
+      if ((st = dd_exchange16(dd, sq, true))) return st;
+      for (int part = 1; part <= 2; part++) {
+        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+        for (int s = 0; s < n; s++) {
+          bqcdg_ctx* c = dd->slabs[s];
+          launch_dd16_pass1(c->g, dd->geom(s), true, part, st_[s], sq[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+                            dd->stream);
+        }
+      }
+      // pass 4: A p, r -= alpha A p, |r|^2 -> the CG step
+      if ((st = dd_exchange16(dd, st_, true))) return st;
+      for (int part = 1; part <= 2; part++) {
+        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+        for (int s = 0; s < n; s++) {
+          bqcdg_ctx* c = dd->slabs[s];
+          launch_dd16_pass4(c->g, dd->geom(s), part, st_[s], sq[s], gauge_of(c, P), aee_of(c, P), op, rs[s],
+                            c->red.partial, part == 1 ? 0 : nsb1, dcg, dd->stream);
+        }
+      }
+      CKL();
+      if ((st = dd_reduce(dd, nsb, dcg, 2))) return st;
+      // x += alpha p of this iteration if it ran, p = r + beta p if the solve goes on
+      for (int s = 0; s < n; s++)
+        launch_cg_pupdate(P, dd->slabs[s]->g, sp[s], rs[s], dcg, dd->stream, 1, xs[s], iter0 + k + 1);
+      CKL();
+      launches += 4 * n + 8 * n + 2 * (dd->nccl ? 2 : 1) + n;
+    }
+    if ((st = get())) return st;
+    if (batch < 16) batch *= 2;
+    if (h.done == 4) break;
+    if (h.done == 0) continue;
+    // reliable update: x += x_s, r = b - A x in FP64 over the slabs
+    const bool periodic = !(h.rtr < h.delta2 * h.maxr2);
+    for (int s = 0; s < n; s++) launch_accum_x(dd->slabs[s]->g, vx[s], (float4*)xs[s].v, dd->stream);
+    CKL();
+    if ((st = residual(rb))) return st;
+    ru++;
+    const double rtrue = rb[0];
+    if (!(rtrue == rtrue)) { h.done = 4; break; }
+    if (rtrue <= stop) { h.rtr = rtrue; converged = true; h.done = 1; break; }
+    if (h.done == 3) { h.rtr = rtrue; break; }
+    if (rtrue < 0.5 * best) { best = rtrue; stall = 0; }
+    else if (++stall >= 5 || rtrue > 1e4 * best) { h.rtr = rtrue; stalled = true; break; }
+    forced = periodic ? forced + 1 : 0;
+    if (forced >= 2) { h.rtr = rtrue; stalled = true; break; }
+    // continue from the true residual with p re-orthogonalised against it
+    for (int s = 0; s < n; s++) {
+      bqcdg_ctx* c = dd->slabs[s];
+      launch_rdot(c->g, rs[s], P, sp[s], c->red, c->dres, dd->stream);
+    }
+    CKL();
+    double rp;
+    if ((st = dd_global_sum(dd, 1, &rp))) return st;
+    const double rpc = rp / rtrue;
+    h.beta = rtrue / h.rtr_old;
+    h.rtr = rtrue;
+    h.maxr2 = rtrue;
+    h.last_ru = h.iter;
+    h.done = 0;
+    if ((st = put())) return st;
+    for (int s = 0; s < n; s++) launch_p_reorth(dd->slabs[s]->g, P, sp[s], rs[s], rpc, h.beta, dd->stream);
+    CKL();
+  }
+  CK(cudaEventRecord(e1, dd->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if ((st = dd_download(dd, vx, x))) return st;
+  info->seconds = ms * 1e-3;
+  info->niter = h.iter;
+  info->reliable_updates = ru;
+  info->kernel_launches = launches;
+  info->rtr = h.rtr;
+  info->true_rtr = h.rtr;
+  info->converged = converged ? 1 : 0;
+  if (h.done == 4) return BQCDG_ENAN;
+  if (stalled || !converged) return BQCDG_ENOCONV;
   return BQCDG_OK;
 }
 

@@ -73,6 +73,13 @@ __host__ __device__ __forceinline__ int dd_tneighbour(const Geom& g, const DdGeo
   return t == 0 ? -1 - i : i - d.V3h;
 }
 
+// the block partials of one reduction on each slab of this process, summed
+// in slab order by the mixed-precision solver's reduction kernel
+constexpr int kMaxDdSlabs = 16;
+struct DdPartials {
+  const double* p[kMaxDdSlabs];
+};
+
 // Overlap of the exchange with the slab's interior: a pass runs as two
 // launches, the interior slices 1 .. Lt_loc-2 (no ghost read) while the faces
 // travel, then the boundary slices 0 and Lt_loc-1.  dd_part_sites: sites of

@@ -407,6 +407,16 @@ int bqcdg_dd_op(bqcdg_dd *dd, int which, double *out, const double *in, const bq
  * FP64, x the initial guess, |r|^2 <= cgp->rest, W = M~ + p->rho */
 int bqcdg_dd_cg(bqcdg_dd *dd, double *x, const double *b, const bqcdg_params *p, const bqcdg_cg_para *cgp,
                 int *iterations, bqcdg_solve_info *info);
+/* (W^+W) x = b on the decomposed lattice with the mixed-precision scheme of
+ * bqcdg_solve (o->precision must be BQCDG_PREC_HALF: int16 iterations, FP32
+ * r and x_s, FP64 reliable updates), x the initial guess; stop as in
+ * bqcdg_solve (o->relative: |r|/|b| <= o->tol, else |r|^2 <= o->tol), the
+ * last residual recomputed in FP64.  The CG scalars stay on the device: the
+ * two reductions of an iteration are summed over the slabs of the process in
+ * slab order and over the ranks by ncclAllReduce.  BQCDG_ENOCONV when the
+ * int16 iterations stop making progress or maxiter is reached. */
+int bqcdg_dd_solve(bqcdg_dd *dd, double *x, const double *b, const bqcdg_params *p, const bqcdg_solver_opts *o,
+                   bqcdg_solve_info *info);
 
 /* ---- allocation-free operator ------------------------------------------- */
 /* This entry point has no counterpart in the reference.  It is for callers

@@ -81,3 +81,29 @@ def test_decomposed_cg_no_convergence_semantics(setup, bq):
     x, it, info = dd.cg(np.zeros_like(b), b, para, rest=1e-30, maxiter=3, log=2)
     assert it == 3 and info.converged == 0
 
+
+
+@pytest.mark.parametrize("rho", [0.0, 0.1])
+def test_decomposed_mixed_solve(setup, bq, rho):
+    """bqcdg_dd_solve: int16 slab passes with FP32 ghost faces, FP64 reliable
+    updates, the two reductions of an iteration summed over the slabs on the
+    device.  The solution must reach a true |b - A x|/|b| < 1e-10 measured by
+    the oracle's operator, and agree with the single-domain mixed solve of the
+    same system (solution to 1e-8, iterations within 15 %)."""
+    g, dd = setup["g"], setup["dd"]
+    kappa, csw = setup["kappa"], setup["csw"]
+    para = bq.HmcPara(kappa=kappa, csw=csw, rho=rho)
+    b = g.gauss_spinor(0)
+    x, info = dd.solve(np.zeros_like(b), b, para, tol=1e-10)
+    assert info.converged, info.as_dict()
+    name = "w_dagger_w" if rho else "mtdagmt"
+    ax = g.op(name, x, setup["uf"], setup["clov"], kappa, csw * kappa, 0.0, rho)
+    assert rel(ax, b) < 1e-10
+    with bq.Lattice(g.L, (1, 1, 1, -1)) as lat:
+        lat.load_gauge(setup["uf"], flipped=True)
+        lat.load_clover(*setup["clov"])
+        x1, i1 = lat.solve(np.zeros_like(b), b, para, precision=bq.PREC_HALF, tol=1e-10)
+    print("slabs %d: %d iterations (%d reliable updates) against %d on one domain"
+          % (dd.nranks, info.niter, info.reliable_updates, i1.niter))
+    assert abs(info.niter - i1.niter) <= max(8, 0.15 * i1.niter)
+    assert rel(x, x1) < 1e-8
