@@ -192,9 +192,9 @@ def build_system(bq, L, device, seed_skip, cool):
 
 # DRAM bytes (read + write) of one k_pass1<int16> launch per output site, from
 # one ncu capture at 32x32x32x32 (dram__bytes_read.sum + dram__bytes_write.sum
-# = 207.3 + 22.2 MB for 524288 sites); traffic grows with the number of
+# = 205.6 + 5.2 MB for 524288 sites); traffic grows with the number of
 # sites, so the per-launch figure at another volume is this times volh
-TRAFFIC_PER_SITE_INT16 = 437.6
+TRAFFIC_PER_SITE_INT16 = 402.0
 
 
 def stencil_bytes_per_site(prec, rec12=True):
@@ -845,6 +845,68 @@ def run_refjob(args, name):
         pg.destroy_process_group()
 
 
+def run_slabs(args):
+    """Optional workload: the benchmark system (32^3x64, the default line's
+    solve) by the mixed-precision CG on the time-slab decomposition
+    (bqcdg_dd_solve) with 1, 2 and 4 slabs, all in this process on one GPU,
+    against the single-domain solve.  What the decomposition costs: the face
+    packing and exchange (device copies here, NCCL messages between GPUs),
+    the split interior/boundary launches and the sums over the slabs.  One
+    step = one solve from x = 0; device seconds by CUDA events."""
+    import numpy as np
+    import bqcdg as bq
+
+    world, rank, local, pg = dist_init()
+    L = lattice_of(args, "32,32,32,64")
+    lat, hb, _ = build_system(bq, L, local, 1000003 * rank, args.cool)
+    para = bq.HmcPara(kappa=KAPPA, csw=CSW)
+    b = lat.field_get(hb)
+    uf = lat.get_gauge(flipped=True)
+    a, ai, _ = lat.get_clover()
+    zero = np.zeros_like(b)
+    bnorm = np.linalg.norm(b)
+
+    def timed(solve):
+        for _ in range(args.warmup):
+            solve()
+        runs = [solve() for _ in range(args.steps)]
+        x, info = runs[-1]
+        res = np.linalg.norm(b - lat.mtdagmt(x, para)) / bnorm   # FP64 residual on the whole lattice
+        return {"seconds": round(sum(r[1].seconds for r in runs) / len(runs), 4), "iterations": info.niter,
+                "reliable_updates": info.reliable_updates, "true_rel_residual": float(res),
+                "converged": bool(info.converged and res < args.tol)}
+
+    one = timed(lambda: lat.solve(zero, b, para, precision=bq.PREC_HALF, tol=args.tol))
+    slabs = {}
+    for n in (1, 2, 4):
+        if L[3] % n or (L[3] // n) % 2:
+            continue
+        with bq.SlabDecomposition.local(L, n) as dd:
+            dd.load_gauge(uf, flipped=True)
+            dd.load_clover(a, ai)
+            slabs[n] = timed(lambda: dd.solve(zero, b, para, tol=args.tol))
+        print("slabs: %d slab(s) %.4f s, %d iterations" % (n, slabs[n]["seconds"], slabs[n]["iterations"]),
+              file=sys.stderr, flush=True)
+    if rank == 0:
+        nmax = max(slabs)
+        out = {"metric": "mixed-precision M^+M CG time-to-1e-10 at %s on %d time slabs of one GPU"
+                         % ("x".join(map(str, L)), nmax),
+               "value": slabs[nmax]["seconds"], "unit": "s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": round(1e3 * slabs[nmax]["seconds"], 1),
+               "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64 (int16 sloppy iterations)",
+               "data": "synthetic: the default workload's system (plaquette %.4f), Gaussian b" % (1.0 - lat.plaq_energy()),
+               "config": {"workload": "bqcdg_dd_solve, lattice %s, kappa %.4f, c_sw %.4f, slabs in one process"
+                                      % ("x".join(map(str, L)), KAPPA, CSW), "parallelism": "replicas x%d" % world},
+               "single_domain": one,
+               "slabs": {str(k): dict(v, overhead_vs_single_domain=round(v["seconds"] / one["seconds"] - 1.0, 4))
+                         for k, v in slabs.items()}}
+        print(json.dumps(out))
+    lat.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def run_confio(args):
     """Optional workload: BQCD's configuration files (conf.F90 conf_write /
     conf_read with the per-slice cksum of cksum.c) for the 32^3x64 links of
@@ -970,10 +1032,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="solve",
-                    choices=["solve", "hmc", "batch", "shifts", "confio", "smp", "mpp", "plumbing"],
+                    choices=["solve", "hmc", "batch", "shifts", "confio", "slabs", "smp", "mpp", "plumbing"],
                     help="solve: the M^+M CG time-to-solution (the default line); hmc: full trajectories; "
                          "batch: 16 right-hand sides; shifts: 8 shifted systems at 64^3x128; "
-                         "confio: configuration files; smp, mpp: the reference's benchmark jobs; "
+                         "confio: configuration files; slabs: the solve on 1, 2, 4 time slabs of one GPU; "
+                         "smp, mpp: the reference's benchmark jobs; "
                          "plumbing: CPU stand-in for testing the multi-process launch")
     ap.add_argument("--therm", type=int, default=10,
                     help="hmc, batch, shifts: forced-accept pure-gauge trajectories on the start configuration")
@@ -1009,6 +1072,8 @@ def main():
         run_shifts(args)
     elif args.workload == "confio":
         run_confio(args)
+    elif args.workload == "slabs":
+        run_slabs(args)
     elif args.workload in REF_JOBS:
         run_refjob(args, args.workload)
     else:

@@ -140,8 +140,7 @@ int dd_check(bqcdg_dd* dd) { return dd && !dd->slabs.empty() ? BQCDG_OK : BQCDG_
 // the faces of field f[s] of every slab, for passes with (dag) or without
 // the dagger, into the ghost buffers of their neighbours: queued on xstream
 // after everything queued so far on the compute stream (which includes the
-// last reads of the ghosts this overwrites); dd_wait_exchange makes the
-// compute stream wait for it
+// last reads of the ghosts this overwrites)
 int dd_exchange(bqcdg_dd* dd, const std::vector<double2*>& f, bool dag) {
   const int n = dd->nslabs();
   CK(cudaEventRecord(dd->ev_ready, dd->stream));
@@ -166,6 +165,12 @@ int dd_exchange(bqcdg_dd* dd, const std::vector<double2*>& f, bool dag) {
     if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclDouble, prev, dd->comm, dd->xstream);
     if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
   }
+  return BQCDG_OK;
+}
+// the boundary launches that read the ghosts are queued on xstream after the
+// exchange; then dd_exchange_done marks the end of the exchange stream's
+// work, and dd_wait_exchange joins it into the compute stream
+int dd_exchange_done(bqcdg_dd* dd) {
   CK(cudaEventRecord(dd->ev_done, dd->xstream));
   return BQCDG_OK;
 }
@@ -201,7 +206,6 @@ int dd_exchange16(bqcdg_dd* dd, const std::vector<SpinorPtr>& f, bool dag) {
     if (e == ncclSuccess) e = g_nccl.recv(b.ghost_bwd, cnt, ncclFloat, prev, dd->comm, dd->xstream);
     if (g_nccl.groupEnd() != ncclSuccess || e != ncclSuccess) return BQCDG_ECUDA;
   }
-  CK(cudaEventRecord(dd->ev_done, dd->xstream));
   return BQCDG_OK;
 }
 
@@ -275,26 +279,27 @@ double2* ainv_oo_of_slab(bqcdg_ctx* c) { return c->Ainv[1]; }
 // out = mtil / mtil_dag in on every slab (t: odd work field of each slab)
 int dd_mtil(bqcdg_dd* dd, bool dag, const std::vector<double2*>& out, const std::vector<double2*>& in,
             const std::vector<double2*>& t, const OpParams& op) {
+  // the boundary slices on the exchange stream behind the faces, the
+  // interior on the compute stream meanwhile, then the join
   int st;
   if ((st = dd_exchange(dd, in, dag))) return st;
-  for (int part = 1; part <= 2; part++) {  // interior while the faces travel, then the boundary slices
-    if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+  for (int part = 2; part >= 1; part--)
     for (int s = 0; s < dd->nslabs(); s++) {
       bqcdg_ctx* c = dd->slabs[s];
-      launch_dd_pass1(c->g, dd->geom(s), dag, t[s], in[s], c->gauge64, ainv_oo_of_slab(c), op, dd->stream, part);
+      launch_dd_pass1(c->g, dd->geom(s), dag, t[s], in[s], c->gauge64, ainv_oo_of_slab(c), op,
+                      part == 2 ? dd->xstream : dd->stream, part);
     }
-  }
   CKL();
+  if ((st = dd_exchange_done(dd)) || (st = dd_wait_exchange(dd))) return st;
   if ((st = dd_exchange(dd, t, dag))) return st;
-  for (int part = 1; part <= 2; part++) {
-    if (part == 2 && (st = dd_wait_exchange(dd))) return st;
+  for (int part = 2; part >= 1; part--)
     for (int s = 0; s < dd->nslabs(); s++) {
       bqcdg_ctx* c = dd->slabs[s];
-      launch_dd_pass2(c->g, dd->geom(s), dag, out[s], t[s], in[s], c->gauge64, aee_of_slab(c), op, dd->stream,
-                      part);
+      launch_dd_pass2(c->g, dd->geom(s), dag, out[s], t[s], in[s], c->gauge64, aee_of_slab(c), op,
+                      part == 2 ? dd->xstream : dd->stream, part);
     }
-  }
   CKL();
+  if ((st = dd_exchange_done(dd)) || (st = dd_wait_exchange(dd))) return st;
   return BQCDG_OK;
 }
 
@@ -496,7 +501,8 @@ int bqcdg_dd_op(bqcdg_dd* dd, int which, double* out, const double* in, const bq
     case 1: case 4: st = dd_mtil(dd, true, vout, vin, t, op); break;
     case 2: case 5: st = dd_mdagm(dd, vout, vin, t, q, op); break;
     default:  // 6: d(EVEN, ODD), 7: d_dag(EVEN, ODD)
-      if ((st = dd_exchange(dd, vin, which == 7)) || (st = dd_wait_exchange(dd))) break;
+      if ((st = dd_exchange(dd, vin, which == 7)) || (st = dd_exchange_done(dd)) || (st = dd_wait_exchange(dd)))
+        break;
       for (int s = 0; s < dd->nslabs(); s++)
         launch_dd_dslash(dd->slabs[s]->g, dd->geom(s), 0, which == 7, vout[s], vin[s], dd->slabs[s]->gauge64,
                          dd->stream);
@@ -596,9 +602,11 @@ int bqcdg_dd_cg(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p,
 // The mixed-precision solve over the slabs: the scheme of cg_core (capi.cu)
 // -- int16 sloppy iterations, FP32 r and x_s, FP64 reliable updates when |r|
 // has fallen by o->delta, p re-orthogonalised after each -- with every
-// stencil pass split around the face exchange and the two reductions of an
-// iteration summed over all slabs (dd_reduce) into one set of CG scalars on
-// the device, so the iterations never wait for the host.
+// stencil pass split around the face exchange (the boundary slices behind
+// the faces on the exchange stream, the interior on the compute stream) and
+// the two reductions of an iteration summed over all slabs (dd_reduce) into
+// one set of CG scalars on the device, so the iterations never wait for the
+// host.
 int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p, const bqcdg_solver_opts* o,
                    bqcdg_solve_info* info) {
   int st = dd_check(dd);
@@ -682,6 +690,18 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
     return BQCDG_OK;
   };
   if ((st = put())) return st;
+  // one stencil pass: the faces of xf exchanged on xstream and the boundary
+  // slices queued behind them there, the interior slices on the compute
+  // stream meanwhile, then the join
+  auto pass = [&](const std::vector<SpinorPtr>& xf, bool dag, auto launch_part) -> int {
+    int s2 = dd_exchange16(dd, xf, dag);
+    if (s2) return s2;
+    for (int part = 2; part >= 1; part--)
+      for (int s = 0; s < n; s++) launch_part(s, part, part == 2 ? dd->xstream : dd->stream);
+    CKL();
+    if ((s2 = dd_exchange_done(dd)) || (s2 = dd_wait_exchange(dd))) return s2;
+    return BQCDG_OK;
+  };
   const int nsb1 = nblocks(dd_part_sites(1, dd->Lt_loc, dd->V3h));
   const int nsb = nsb1 + nblocks(dd_part_sites(2, dd->Lt_loc, dd->V3h));
   int batch = 4, ru = 0, stall = 0, forced = 0, launches = 0;
@@ -691,49 +711,33 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
     const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
       // pass 1: t = A_oo^-1 D_oe p
-      if ((st = dd_exchange16(dd, sp, false))) return st;
-      for (int part = 1; part <= 2; part++) {
-        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
-        for (int s = 0; s < n; s++) {
-          bqcdg_ctx* c = dd->slabs[s];
-          launch_dd16_pass1(c->g, dd->geom(s), false, part, st_[s], sp[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
-                            dd->stream);
-        }
-      }
+      st = pass(sp, false, [&](int s, int part, cudaStream_t str) {
+        bqcdg_ctx* c = dd->slabs[s];
+        launch_dd16_pass1(c->g, dd->geom(s), false, part, st_[s], sp[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+                          str);
+      });
+      if (st) return st;
       // pass 2: q = M~ p, |q|^2 -> alpha
-      if ((st = dd_exchange16(dd, st_, false))) return st;
-      for (int part = 1; part <= 2; part++) {
-        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
-        for (int s = 0; s < n; s++) {
-          bqcdg_ctx* c = dd->slabs[s];
-          launch_dd16_pass2(c->g, dd->geom(s), false, part, sq[s], st_[s], sp[s], gauge_of(c, P), aee_of(c, P), op,
-                            c->red.partial, part == 1 ? 0 : nsb1, dcg, dd->stream);
-        }
-      }
-      CKL();
-      if ((st = dd_reduce(dd, nsb, dcg, 1))) return st;
+      st = pass(st_, false, [&](int s, int part, cudaStream_t str) {
+        bqcdg_ctx* c = dd->slabs[s];
+        launch_dd16_pass2(c->g, dd->geom(s), false, part, sq[s], st_[s], sp[s], gauge_of(c, P), aee_of(c, P), op,
+                          c->red.partial, part == 1 ? 0 : nsb1, dcg, str);
+      });
+      if (st || (st = dd_reduce(dd, nsb, dcg, 1))) return st;
       // pass 3: t = A_oo^-1 D^+_oe q
-      if ((st = dd_exchange16(dd, sq, true))) return st;
-      for (int part = 1; part <= 2; part++) {
-        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
-        for (int s = 0; s < n; s++) {
-          bqcdg_ctx* c = dd->slabs[s];
-          launch_dd16_pass1(c->g, dd->geom(s), true, part, st_[s], sq[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
-                            dd->stream);
-        }
-      }
+      st = pass(sq, true, [&](int s, int part, cudaStream_t str) {
+        bqcdg_ctx* c = dd->slabs[s];
+        launch_dd16_pass1(c->g, dd->geom(s), true, part, st_[s], sq[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+                          str);
+      });
+      if (st) return st;
       // pass 4: A p, r -= alpha A p, |r|^2 -> the CG step
-      if ((st = dd_exchange16(dd, st_, true))) return st;
-      for (int part = 1; part <= 2; part++) {
-        if (part == 2 && (st = dd_wait_exchange(dd))) return st;
-        for (int s = 0; s < n; s++) {
-          bqcdg_ctx* c = dd->slabs[s];
-          launch_dd16_pass4(c->g, dd->geom(s), part, st_[s], sq[s], gauge_of(c, P), aee_of(c, P), op, rs[s],
-                            c->red.partial, part == 1 ? 0 : nsb1, dcg, dd->stream);
-        }
-      }
-      CKL();
-      if ((st = dd_reduce(dd, nsb, dcg, 2))) return st;
+      st = pass(st_, true, [&](int s, int part, cudaStream_t str) {
+        bqcdg_ctx* c = dd->slabs[s];
+        launch_dd16_pass4(c->g, dd->geom(s), part, st_[s], sq[s], gauge_of(c, P), aee_of(c, P), op, rs[s],
+                          c->red.partial, part == 1 ? 0 : nsb1, dcg, str);
+      });
+      if (st || (st = dd_reduce(dd, nsb, dcg, 2))) return st;
       // x += alpha p of this iteration if it ran, p = r + beta p if the solve goes on
       for (int s = 0; s < n; s++)
         launch_cg_pupdate(P, dd->slabs[s]->g, sp[s], rs[s], dcg, dd->stream, 1, xs[s], iter0 + k + 1);
