@@ -628,15 +628,15 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
   if ((st = dd_fields(dd, 0, vx)) || (st = dd_fields(dd, 1, vb)) || (st = dd_fields(dd, 2, vr)) ||
       (st = dd_fields(dd, 3, vax)) || (st = dd_fields(dd, 4, t64)) || (st = dd_fields(dd, 5, q64)))
     return st;
-  std::vector<SpinorPtr> sp(n), st_(n), sq(n), rs(n), xs(n);
+  std::vector<SpinorPtr> sp(n), tf(n), sq(n), rs(n), xs(n);
   for (int s = 0; s < n; s++) {
     bqcdg_ctx* c = dd->slabs[s];
     sp[s] = c->sp(P, 0);
-    st_[s] = c->sp(P, 1);
+    tf[s] = c->sp(P, 1);
     sq[s] = c->sp(P, 2);
     rs[s] = c->sp(Prec::F32, 0);
     xs[s] = c->sp(Prec::F32, 1);
-    if (!sp[s].v || !st_[s].v || !sq[s].v || !rs[s].v || !xs[s].v) return BQCDG_ENOMEM;
+    if (!sp[s].v || !tf[s].v || !sq[s].v || !rs[s].v || !xs[s].v) return BQCDG_ENOMEM;
   }
   if ((st = dd_upload(dd, x, vx)) || (st = dd_upload(dd, b, vb))) return st;
   const OpParams op = op_of(p, true);
@@ -703,6 +703,7 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
     return BQCDG_OK;
   };
   const int nsb1 = nblocks(dd_part_sites(1, dd->Lt_loc, dd->V3h));
+  const int nparts = nsb1 > 0 ? 2 : 1;  // a slab of two slices has no interior launch
   const int nsb = nsb1 + nblocks(dd_part_sites(2, dd->Lt_loc, dd->V3h));
   int batch = 4, ru = 0, stall = 0, forced = 0, launches = 0;
   double best = rb[0];
@@ -713,28 +714,28 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
       // pass 1: t = A_oo^-1 D_oe p
       st = pass(sp, false, [&](int s, int part, cudaStream_t str) {
         bqcdg_ctx* c = dd->slabs[s];
-        launch_dd16_pass1(c->g, dd->geom(s), false, part, st_[s], sp[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+        launch_dd16_pass1(c->g, dd->geom(s), false, part, tf[s], sp[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
                           str);
       });
       if (st) return st;
       // pass 2: q = M~ p, |q|^2 -> alpha
-      st = pass(st_, false, [&](int s, int part, cudaStream_t str) {
+      st = pass(tf, false, [&](int s, int part, cudaStream_t str) {
         bqcdg_ctx* c = dd->slabs[s];
-        launch_dd16_pass2(c->g, dd->geom(s), false, part, sq[s], st_[s], sp[s], gauge_of(c, P), aee_of(c, P), op,
+        launch_dd16_pass2(c->g, dd->geom(s), false, part, sq[s], tf[s], sp[s], gauge_of(c, P), aee_of(c, P), op,
                           c->red.partial, part == 1 ? 0 : nsb1, dcg, str);
       });
       if (st || (st = dd_reduce(dd, nsb, dcg, 1))) return st;
       // pass 3: t = A_oo^-1 D^+_oe q
       st = pass(sq, true, [&](int s, int part, cudaStream_t str) {
         bqcdg_ctx* c = dd->slabs[s];
-        launch_dd16_pass1(c->g, dd->geom(s), true, part, st_[s], sq[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
+        launch_dd16_pass1(c->g, dd->geom(s), true, part, tf[s], sq[s], gauge_of(c, P), ainv_of(c, P), op, dcg,
                           str);
       });
       if (st) return st;
       // pass 4: A p, r -= alpha A p, |r|^2 -> the CG step
-      st = pass(st_, true, [&](int s, int part, cudaStream_t str) {
+      st = pass(tf, true, [&](int s, int part, cudaStream_t str) {
         bqcdg_ctx* c = dd->slabs[s];
-        launch_dd16_pass4(c->g, dd->geom(s), part, st_[s], sq[s], gauge_of(c, P), aee_of(c, P), op, rs[s],
+        launch_dd16_pass4(c->g, dd->geom(s), part, tf[s], sq[s], gauge_of(c, P), aee_of(c, P), op, rs[s],
                           c->red.partial, part == 1 ? 0 : nsb1, dcg, str);
       });
       if (st || (st = dd_reduce(dd, nsb, dcg, 2))) return st;
@@ -742,7 +743,7 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
       for (int s = 0; s < n; s++)
         launch_cg_pupdate(P, dd->slabs[s]->g, sp[s], rs[s], dcg, dd->stream, 1, xs[s], iter0 + k + 1);
       CKL();
-      launches += 4 * n + 8 * n + 2 * (dd->nccl ? 2 : 1) + n;
+      launches += 4 * (n + nparts * n) + 2 * (dd->nccl ? 2 : 1) + n;
     }
     if ((st = get())) return st;
     if (batch < 16) batch *= 2;

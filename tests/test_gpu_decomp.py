@@ -83,21 +83,21 @@ def test_decomposed_cg_no_convergence_semantics(setup, bq):
 
 
 
-@pytest.mark.parametrize("rho", [0.0, 0.1])
-def test_decomposed_mixed_solve(setup, bq, rho):
+@pytest.mark.parametrize("rho,clover", [(0.0, True), (0.1, True), (0.0, False)], ids=["mtdagmt", "w_dagger_w", "wilson"])
+def test_decomposed_mixed_solve(setup, bq, rho, clover):
     """bqcdg_dd_solve: int16 slab passes with FP32 ghost faces, FP64 reliable
     updates, the two reductions of an iteration summed over the slabs on the
     device.  The solution must reach a true |b - A x|/|b| < 1e-10 measured by
     the oracle's operator, and agree with the single-domain mixed solve of the
     same system (solution to 1e-8, iterations within 15 %)."""
     g, dd = setup["g"], setup["dd"]
-    kappa, csw = setup["kappa"], setup["csw"]
+    kappa, csw = setup["kappa"], (setup["csw"] if clover else 0.0)
     para = bq.HmcPara(kappa=kappa, csw=csw, rho=rho)
     b = g.gauss_spinor(0)
     x, info = dd.solve(np.zeros_like(b), b, para, tol=1e-10)
     assert info.converged, info.as_dict()
     name = "w_dagger_w" if rho else "mtdagmt"
-    ax = g.op(name, x, setup["uf"], setup["clov"], kappa, csw * kappa, 0.0, rho)
+    ax = g.op(name, x, setup["uf"], setup["clov"] if clover else None, kappa, csw * kappa, 0.0, rho)
     assert rel(ax, b) < 1e-10
     with bq.Lattice(g.L, (1, 1, 1, -1)) as lat:
         lat.load_gauge(setup["uf"], flipped=True)
