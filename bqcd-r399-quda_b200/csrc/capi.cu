@@ -236,10 +236,12 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     const int iter0 = h.iter;
     for (int k = 0; k < batch; k++) {
       // pass 1, pass 2 (+|M~p|^2 partials), pass 3 (+ their sum -> alpha), pass 4 (+x,r update, |r|^2
-      // partials), the CG step, p update.  With time_kernels, passes 1 and 3 of the first iteration of
-      // each batch are bracketed by events: a sample of every batch, and events between all launches
-      // would lengthen the solve they time.
-      const bool timed = k == 0;
+      // partials), the CG step, p update.  With time_kernels, passes 1 and 3 of the second iteration of
+      // each batch are bracketed by events: a sample of every batch in the steady state (the first
+      // iteration follows the host's read of the scalars, or a reliable update whose FP64 fields have
+      // displaced the int16 ones from L2), and events between all launches would lengthen the solve
+      // they time.
+      const bool timed = k == 1;
       if (timed) kt.begin();
       launch_mtil_pass1(sloppy, gs, false, t, p, gauge_of(c, sloppy), ainv_of(c, sloppy), op, c->dcg, c->stream);
       if (timed) kt.end();
@@ -257,7 +259,7 @@ int cg_core(bqcdg_ctx* c, double2* x, double2* b, const OpParams& op, Prec slopp
     CKL();
     int st = read_cg(c);
     if (st) return st;
-    kt.collect(h.iter > iter0 ? 2 : 0);  // the two timed passes ran if the batch's first iteration did
+    kt.collect(h.iter > iter0 + 1 ? 2 : 0);  // the two timed passes ran if the batch's second iteration did
     if (batch < 16) batch *= 2;
     if (h.done == 4) break;
     if (h.done == 0) continue;

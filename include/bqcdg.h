@@ -79,7 +79,7 @@ typedef struct {
   double tol;
   double delta;       /* reliable update when |r| < delta * max|r| since the last one */
   int check_true_residual; /* 1: recompute |b - A x|^2 in FP64 at the end */
-  int time_kernels;   /* 1: time the first-half stencil launches of the first
+  int time_kernels;   /* 1: time the first-half stencil launches of the second
                          iteration of every batch of queued iterations with
                          CUDA events (FP64 and single-RHS sloppy solves) */
   int rhs_per_thread; /* batched solves: right-hand sides each stencil thread serves
