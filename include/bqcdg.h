@@ -375,7 +375,9 @@ int bqcdg_field_cdot_pairs(bqcdg_ctx *ctx, int n, const int *ha, const int *hb, 
  * rank+1, and the CG takes the global sums of its three scalars, as the
  * reference's MPI build does (d/D21.F90:53-72, comm/xbound_mpi.F90:418-461,
  * cg.F90:91,97,109).  U_t of each slab's last slice is sent to rank+1 once per
- * gauge field.  Everything here is FP64.
+ * gauge field.  The operators and bqcdg_dd_cg are FP64; bqcdg_dd_solve runs
+ * int16 iterations with FP32 faces and FP64 reliable updates.  The faces go
+ * on a second stream while the slab interior computes.
  *
  * Two ways to run it:
  *  - bqcdg_dd_create_local: all nranks slabs in this process on one device,
@@ -386,7 +388,9 @@ int bqcdg_field_cdot_pairs(bqcdg_ctx *ctx, int n, const int *ha, const int *hb, 
  *    stream.  Rank 0 makes the id with bqcdg_dd_nccl_unique_id and hands its
  *    128 bytes to the others (any side channel).  Host arrays are the slab's
  *    own (volh = V3h Lt sites per parity).  libnccl.so.2 is opened at run
- *    time; without it both calls return BQCDG_EUNSUPPORTED. */
+ *    time; without it both calls return BQCDG_EUNSUPPORTED.  Every call
+ *    that exchanges or sums (load_gauge, op, cg, solve) is collective: all
+ *    ranks make it, in the same order and with the same parameters. */
 typedef struct bqcdg_dd bqcdg_dd;
 int bqcdg_dd_create_local(bqcdg_dd **dd, const int L[4], const int bc[4], int nranks, int device);
 int bqcdg_dd_nccl_unique_id(char *id128);
