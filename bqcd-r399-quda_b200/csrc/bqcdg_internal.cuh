@@ -1163,7 +1163,8 @@ __device__ __forceinline__ bool last_block(unsigned int* counter, int nsb) {
 
 template <int N>
 __device__ __forceinline__ void final_sum(const double* partial, int nblocks_stride, int nsb, double (&out)[N]) {
-  // executed by the whole last block: warp-parallel fixed-order sum.  Each
+  // executed by a whole block (the last to arrive, or the block that sums
+  // another launch's partials): warp-parallel fixed-order sum.  Each
   // thread keeps 8 loads in flight (8 running sums, combined in a fixed
   // order), so the tail that the rest of the GPU waits for costs a few L2
   // latencies rather than one per partial.

@@ -53,7 +53,8 @@ __device__ __forceinline__ CloverView<Prec::F16> cview<Prec::F16>(CloverPtr p, i
 
 // the scalar part of one CG iteration once |r|^2 of the new residual is
 // known (cg.F90:107-116), with the stop and reliable-update decisions of the
-// mixed-precision solver; run by one thread of the last block
+// mixed-precision solver; run by one thread: of k_cg_step in the CG loop, of
+// the last block to arrive where a fused pass takes the step itself
 __device__ __forceinline__ void cg_scalar_step(CgScalars* cg, double rtr) {
   cg->iter += 1;
   cg->rtr_old = cg->rtr;
