@@ -137,6 +137,19 @@ namespace {
 
 int dd_check(bqcdg_dd* dd) { return dd && !dd->slabs.empty() ? BQCDG_OK : BQCDG_EINVAL; }
 
+// the two timing events of a solve, released on every return path
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t create() {
+    cudaError_t e = cudaEventCreate(&e0);
+    return e == cudaSuccess ? cudaEventCreate(&e1) : e;
+  }
+  ~EventPair() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
 // the faces of field f[s] of every slab, for passes with (dag) or without
 // the dagger, into the ghost buffers of their neighbours: queued on xstream
 // after everything queued so far on the compute stream (which includes the
@@ -535,9 +548,9 @@ int bqcdg_dd_cg(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p,
   if ((st = dd_upload(dd, x, vx)) || (st = dd_upload(dd, b, vb))) return st;
   const OpParams op = op_of(p, true);
   const int n = dd->nslabs();
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  EventPair ev;
+  CK(ev.create());
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1;
   CK(cudaEventRecord(e0, dd->stream));
   auto dot = [&](const std::vector<double2*>& a, const std::vector<double2*>& c2, double* out) {
     for (int s = 0; s < n; s++) {
@@ -586,8 +599,6 @@ int bqcdg_dd_cg(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params* p,
   CK(cudaEventSynchronize(e1));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if ((st = dd_download(dd, vx, x))) return st;
   info->niter = niter;
   info->rtr = rtr;
@@ -642,9 +653,9 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
   const OpParams op = op_of(p, true);
   bqcdg_ctx* c0 = dd->slabs[0];
   CgScalars* dcg = c0->dcg;  // the scalars every slab's kernels read
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  EventPair ev;
+  CK(ev.create());
+  cudaEvent_t e0 = ev.e0, e1 = ev.e1;
   CK(cudaEventRecord(e0, dd->stream));
 
   // r = b - A x in FP64 and |r|^2, |b|^2 over the slabs
@@ -785,8 +796,6 @@ int bqcdg_dd_solve(bqcdg_dd* dd, double* x, const double* b, const bqcdg_params*
   CK(cudaEventSynchronize(e1));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   if ((st = dd_download(dd, vx, x))) return st;
   info->seconds = ms * 1e-3;
   info->niter = h.iter;
