@@ -123,6 +123,9 @@ struct KernelTimer {
   std::vector<cudaEvent_t> pending;
   double ms = 0.0;
   int launches = 0;
+  ~KernelTimer() {  // events left when a solve returns early
+    for (auto e : pending) cudaEventDestroy(e);
+  }
   void begin() {
     if (!on) return;
     cudaEvent_t e;
