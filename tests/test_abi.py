@@ -109,3 +109,23 @@ def test_slab_decomposition_shape_is_checked(bq):
     with pytest.raises(bq.BqcdgError) as e:
         bq.SlabDecomposition.local((8, 8, 8, 12), 4)       # slabs of 3 slices would mix parities
     assert e.value.status == bq.EINVAL
+
+
+def test_slab_solvers_check_their_arguments(so, bq):
+    """bqcdg_dd_cg and bqcdg_dd_solve refuse a missing decomposition or
+    missing arrays before they touch a device."""
+    lib = C.CDLL(so)
+    one = C.c_void_p(1)            # never dereferenced: the checks come first
+    prm = bq.Params(0.13, 0.0, 0.0, 0.0)
+    cgp = bq.CgPara(1e-20, 100, 0)
+    opts = bq.SolverOpts(bq.PREC_HALF, 100, 1, 1e-10, 0.1, 1, 0, 0)
+    info = bq.SolveInfo()
+    it = C.c_int()
+    lib.bqcdg_dd_cg.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(bq.Params), C.POINTER(bq.CgPara),
+                                C.POINTER(C.c_int), C.POINTER(bq.SolveInfo)]
+    lib.bqcdg_dd_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(bq.Params),
+                                   C.POINTER(bq.SolverOpts), C.POINTER(bq.SolveInfo)]
+    assert lib.bqcdg_dd_cg(None, one, one, C.byref(prm), C.byref(cgp), C.byref(it), C.byref(info)) == bq.EINVAL
+    assert lib.bqcdg_dd_solve(None, one, one, C.byref(prm), C.byref(opts), C.byref(info)) == bq.EINVAL
+    assert lib.bqcdg_dd_op(None, 0, one, one, C.byref(prm)) == bq.EINVAL
+    assert lib.bqcdg_dd_volh(None) == -1
